@@ -1,0 +1,136 @@
+/*
+ * planck_fock.h -- C ABI of the B200 direct-SCF Fock-build engine.
+ *
+ * Drop-in for the two-electron part of Planck's SCF: the entry points below
+ * replace the functions callers reach through src/integrals/base.h
+ * (reference project paths):
+ *
+ *   _compute_2e        base.h:39-55   -> pfk_eri_tensor
+ *   _compute_2e_fock   base.h:57-73   -> pfk_fock_rhf   (G = J - K/2)
+ *   _compute_2e_fock_uhf base.h:75-93 -> pfk_fock_uhf   (G_a, G_b)
+ *   build_coulomb_from_eri / build_exchange_from_eri
+ *                      src/dft/driver.cpp:689-731 -> pfk_jk
+ *   _compute_schwarz_table os.cpp:1703-1752 / rys.cpp:509-556 -> pfk_schwarz
+ *   the screened quartet loop os.cpp:1458-1476 -> pfk_quartet_count / _list
+ *
+ * Conventions
+ *   - Basis data is the reference's Shell data (src/base/types.h:263-275):
+ *     centre in Bohr, L, primitive exponents, contraction coefficients with
+ *     the contracted normalisation already folded in (gaussian.cpp:273-281),
+ *     and per-primitive normalisations (basis.cpp:39-48).  Shells appear in
+ *     the reference's order; each shell expands to (L+1)(L+2)/2 Cartesian
+ *     functions ordered lx descending, then ly descending (basis.cpp:20-37),
+ *     with component norms 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!)
+ *     (gaussian.cpp:283-296).  0 <= L <= 3.
+ *   - Matrices are nbasis x nbasis FP64.  Densities must be symmetric (every
+ *     SCF density is); G, J and K come back symmetric, so row- and
+ *     column-major storage coincide (the reference's Eigen matrices are
+ *     column-major).
+ *   - tol_eri screens canonical AO quartets exactly as the reference does:
+ *     a quartet is skipped when Q(i,j)*Q(k,l) < tol_eri, Q = sqrt|(ij|ij)|.
+ *   - Every call returns a status; nothing throws across the ABI.  A failed
+ *     call leaves a message in pfk_last_error(ctx).
+ *   - A context owns its device memory, stream and captured graphs.  It is
+ *     single-threaded; use one context per molecule (several may coexist).
+ */
+#ifndef PLANCK_FOCK_H
+#define PLANCK_FOCK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PFK_OK = 0,
+    PFK_ERR_INVALID = 1,     /* bad argument or basis data */
+    PFK_ERR_UNSUPPORTED = 2, /* e.g. L > 3, non-null symmetry operations */
+    PFK_ERR_CUDA = 3,        /* CUDA runtime error (message in pfk_last_error) */
+    PFK_ERR_NOMEM = 4,       /* device or host allocation failed */
+    PFK_ERR_STATE = 5        /* call out of order (e.g. null context) */
+} pfk_status;
+
+/* IntegralMethod (src/base/types.h:88-100): OS, Rys, Auto. */
+typedef enum { PFK_ENGINE_OS = 0, PFK_ENGINE_RYS = 1, PFK_ENGINE_AUTO = 2 } pfk_engine;
+
+/* FP64 everywhere, or FP32 for quartets whose Schwarz bound is below
+ * fp32_bound (roots/weights, Fock accumulation stay FP64). */
+typedef enum { PFK_PREC_FP64 = 0, PFK_PREC_MIXED = 1 } pfk_precision;
+
+typedef struct {
+    int nshell;
+    const int *L;          /* [nshell] angular momentum, 0..3 */
+    const int *nprim;      /* [nshell] primitives per shell */
+    const double *center;  /* [3*nshell] Bohr */
+    const double *expo;    /* [sum nprim] Shell::_primitives */
+    const double *coef;    /* [sum nprim] Shell::_coefficients (Nc folded in) */
+    const double *norm;    /* [sum nprim] Shell::_normalizations */
+} pfk_basis_desc;
+
+typedef struct pfk_ctx pfk_ctx;
+
+/* Build the context on CUDA device `device`: uploads shell-pair data,
+ * computes the Schwarz table and the screened quartet lists for tol_eri
+ * = 1e-10 (OptionsIntegral default, types.h:408-412).  Replaces the
+ * per-call Schwarz table of os.cpp:1447. */
+pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out);
+pfk_status pfk_destroy(pfk_ctx *ctx);
+
+/* OptionsIntegral (types.h:408-412): tol_eri and engine.  precision and
+ * fp32_bound select the mixed-precision path.  Rebuilds the quartet lists
+ * when tol_eri or fp32_bound change. */
+pfk_status pfk_set_options(pfk_ctx *ctx, double tol_eri, int engine, int precision,
+                           double fp32_bound);
+
+int pfk_nbasis(const pfk_ctx *ctx);
+const char *pfk_last_error(const pfk_ctx *ctx);
+
+/* Schwarz table Q(i,j) = sqrt|(ij|ij)|, nbasis x nbasis, host buffer.
+ * Counterpart of _compute_schwarz_table (os.cpp:1703-1752). */
+pfk_status pfk_schwarz(pfk_ctx *ctx, double *Q);
+
+/* Screened canonical AO quartet set (os.cpp:1458-1476): count, an order-
+ * independent 64-bit digest (sum over quartets of mix64 of the packed
+ * i<<48|j<<32|k<<16|l code with i<=j, k<=l, (i,j)<=(k,l)), and the number
+ * of shell quartets the kernels evaluate. */
+pfk_status pfk_quartet_count(pfk_ctx *ctx, long long *n_ao_quartets, uint64_t *digest,
+                             long long *n_shell_quartets);
+
+/* The AO quartets themselves (4 ints each, canonical, unordered); up to cap. */
+pfk_status pfk_quartet_list(pfk_ctx *ctx, int *out, long long cap, long long *n);
+
+/* RHF: G = J(P) - K(P)/2.  _compute_2e_fock (base.h:57-73, os.cpp:1435-1523). */
+pfk_status pfk_fock_rhf(pfk_ctx *ctx, const double *P, double *G);
+
+/* UHF: Ga = J(Pa+Pb) - K(Pa), Gb = J(Pa+Pb) - K(Pb).
+ * _compute_2e_fock_uhf (base.h:75-93, os.cpp:1533-1625). */
+pfk_status pfk_fock_uhf(pfk_ctx *ctx, const double *Pa, const double *Pb, double *Ga, double *Gb);
+
+/* RKS/UKS Coulomb and exchange: J = J(P), K = k_scale * K(Pk)
+ * (dft/driver.cpp:689-731 builds them from the stored tensor; hybrids scale
+ * K by the exact-exchange fraction).  Pk may equal P; K may be NULL. */
+pfk_status pfk_jk(pfk_ctx *ctx, const double *P, const double *Pk, double *J, double *K,
+                  double k_scale);
+
+/* Device-pointer form of pfk_fock_rhf: dP and dG live on the context's
+ * device; the call is asynchronous on `stream` (a cudaStream_t, NULL for the
+ * context's own stream).  The first call with a given (dP, dG, stream)
+ * captures the whole build in a CUDA graph and later calls replay it. */
+pfk_status pfk_fock_rhf_device(pfk_ctx *ctx, const double *dP, double *dG, void *stream);
+
+/* Conventional build: the full nbasis^4 tensor, row-major
+ * i*nb^3 + j*nb^2 + k*nb + l, all 8 permutations written
+ * (_compute_2e, os.cpp:1755-1829).  Host buffer of nb^4 doubles. */
+pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri);
+
+/* Per-class shell-quartet counts (55 classes (ss|ss)..(ff|ff)) and the
+ * device time of the last build per class in milliseconds, for profiling. */
+pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, double *ms55);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLANCK_FOCK_H */

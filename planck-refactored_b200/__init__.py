@@ -1,0 +1,221 @@
+"""planck-refactored_b200: B200-native direct-SCF Fock build for Planck.
+
+Python host mirror of the reference's two-electron interface
+(src/integrals/base.h:39-93) over the C ABI in include/planck_fock.h.
+The compute path is the CUDA library libplanck_fock.so built in-tree by
+build.py; there is no CPU fallback -- importing works without a GPU, but
+every compute call fails loudly if the library or the device is missing.
+
+Typical use (mirrors scf.cpp:281-284):
+
+    eng = FockEngine(shells)                 # once per geometry
+    G = _compute_2e_fock(eng, P, nbasis, "os", 1e-10)
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .basis import (ANGSTROM_TO_BOHR, Molecule, cartesian_order, component_norm,  # noqa: F401
+                    read_gbs_basis, shells_for)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplanck_fock.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include", "planck_fock.h")
+
+PFK_OK, PFK_ERR_INVALID, PFK_ERR_UNSUPPORTED, PFK_ERR_CUDA, PFK_ERR_NOMEM, PFK_ERR_STATE = range(6)
+ENGINES = {"os": 0, "rys": 1, "auto": 2}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
+           "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
+           "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats"]
+
+_lib = None
+
+
+class PfkError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"pfk status {status}: {msg}")
+        self.status = status
+
+
+class BasisDesc(ctypes.Structure):
+    _fields_ = [("nshell", ctypes.c_int), ("L", ctypes.c_void_p), ("nprim", ctypes.c_void_p),
+                ("center", ctypes.c_void_p), ("expo", ctypes.c_void_p), ("coef", ctypes.c_void_p),
+                ("norm", ctypes.c_void_p)]
+
+
+def load_library(path=LIB_PATH):
+    """Load libplanck_fock.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python build.py` (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    vp, c_int, c_dbl, c_ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+    for name in EXPORTS:
+        getattr(L, name).restype = c_int
+    L.pfk_create.argtypes = [ctypes.POINTER(BasisDesc), c_int, ctypes.POINTER(vp)]
+    L.pfk_destroy.argtypes = [vp]
+    L.pfk_set_options.argtypes = [vp, c_dbl, c_int, c_int, c_dbl]
+    L.pfk_nbasis.argtypes = [vp]
+    L.pfk_last_error.restype = ctypes.c_char_p
+    L.pfk_last_error.argtypes = [vp]
+    L.pfk_schwarz.argtypes = [vp, vp]
+    L.pfk_quartet_count.argtypes = [vp, ctypes.POINTER(c_ll), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(c_ll)]
+    L.pfk_quartet_list.argtypes = [vp, vp, c_ll, ctypes.POINTER(c_ll)]
+    L.pfk_fock_rhf.argtypes = [vp, vp, vp]
+    L.pfk_fock_uhf.argtypes = [vp, vp, vp, vp, vp]
+    L.pfk_jk.argtypes = [vp, vp, vp, vp, vp, c_dbl]
+    L.pfk_fock_rhf_device.argtypes = [vp, vp, vp, vp]
+    L.pfk_eri_tensor.argtypes = [vp, vp]
+    L.pfk_class_stats.argtypes = [vp, vp, vp]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+CLASS_NAMES = []
+for _x in range(10):
+    for _y in range(_x + 1):
+        _pc = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3)]
+        _s = "spdf"
+        CLASS_NAMES.append(f"({_s[_pc[_x][0]]}{_s[_pc[_x][1]]}|{_s[_pc[_y][0]]}{_s[_pc[_y][1]]})")
+
+
+class FockEngine:
+    """One molecule/basis on one GPU: owns a pfk_ctx (device data, screened
+    quartet lists, captured graphs)."""
+
+    def __init__(self, shells, device=0, tol_eri=1e-10, engine="os", precision="fp64", fp32_bound=1e-8):
+        self.lib = load_library()
+        self._keep = {k: np.ascontiguousarray(v) for k, v in shells.items()}
+        s = self._keep
+        s["L"] = np.ascontiguousarray(s["L"], dtype=np.int32)
+        s["nprim"] = np.ascontiguousarray(s["nprim"], dtype=np.int32)
+        for k in ("center", "expo", "coef", "norm"):
+            s[k] = _f64(s[k])
+        desc = BasisDesc(len(s["L"]), _p(s["L"]), _p(s["nprim"]), _p(s["center"]), _p(s["expo"]),
+                         _p(s["coef"]), _p(s["norm"]))
+        h = ctypes.c_void_p()
+        st = self.lib.pfk_create(ctypes.byref(desc), int(device), ctypes.byref(h))
+        if st != PFK_OK:
+            raise PfkError(st, self.lib.pfk_last_error(None).decode())
+        self.h = h
+        self.nbasis = self.lib.pfk_nbasis(h)
+        self.tol_eri, self.engine, self.precision, self.fp32_bound = 1e-10, "os", "fp64", fp32_bound
+        self.set_options(tol_eri, engine, precision, fp32_bound)
+
+    def _check(self, st):
+        if st != PFK_OK:
+            raise PfkError(st, self.lib.pfk_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pfk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_options(self, tol_eri=1e-10, engine="os", precision="fp64", fp32_bound=1e-8):
+        self._check(self.lib.pfk_set_options(self.h, float(tol_eri), ENGINES[engine], PRECISIONS[precision],
+                                             float(fp32_bound)))
+        self.tol_eri, self.engine, self.precision, self.fp32_bound = tol_eri, engine, precision, fp32_bound
+
+    def schwarz(self):
+        Q = np.zeros((self.nbasis, self.nbasis))
+        self._check(self.lib.pfk_schwarz(self.h, _p(Q)))
+        return Q
+
+    def quartet_count(self):
+        n = ctypes.c_longlong()
+        d = ctypes.c_uint64()
+        ns = ctypes.c_longlong()
+        self._check(self.lib.pfk_quartet_count(self.h, ctypes.byref(n), ctypes.byref(d), ctypes.byref(ns)))
+        return n.value, d.value, ns.value
+
+    def quartet_list(self):
+        n_ao, _, _ = self.quartet_count()
+        out = np.zeros((max(n_ao, 1), 4), dtype=np.int32)
+        n = ctypes.c_longlong()
+        self._check(self.lib.pfk_quartet_list(self.h, _p(out), n_ao, ctypes.byref(n)))
+        return out[:n.value]
+
+    def fock_rhf(self, P):
+        P = _f64(P)
+        G = np.zeros_like(P)
+        self._check(self.lib.pfk_fock_rhf(self.h, _p(P), _p(G)))
+        return G
+
+    def fock_uhf(self, Pa, Pb):
+        Pa, Pb = _f64(Pa), _f64(Pb)
+        Ga, Gb = np.zeros_like(Pa), np.zeros_like(Pb)
+        self._check(self.lib.pfk_fock_uhf(self.h, _p(Pa), _p(Pb), _p(Ga), _p(Gb)))
+        return Ga, Gb
+
+    def jk(self, P, Pk=None, k_scale=1.0, want_k=True):
+        P = _f64(P)
+        Pk = P if Pk is None else _f64(Pk)
+        J = np.zeros_like(P)
+        K = np.zeros_like(P) if want_k else None
+        self._check(self.lib.pfk_jk(self.h, _p(P), _p(Pk), _p(J), _p(K) if want_k else None, float(k_scale)))
+        return J, K
+
+    def fock_rhf_device(self, dP_ptr, dG_ptr, stream_ptr=0):
+        self._check(self.lib.pfk_fock_rhf_device(self.h, ctypes.c_void_p(dP_ptr), ctypes.c_void_p(dG_ptr),
+                                                 ctypes.c_void_p(stream_ptr or None)))
+
+    def eri_tensor(self):
+        nb = self.nbasis
+        eri = np.zeros((nb, nb, nb, nb))
+        self._check(self.lib.pfk_eri_tensor(self.h, _p(eri)))
+        return eri
+
+    def class_stats(self, timed=True):
+        q = np.zeros(55, dtype=np.int64)
+        ms = np.zeros(55)
+        self._check(self.lib.pfk_class_stats(self.h, _p(q), _p(ms) if timed else None))
+        return {CLASS_NAMES[c]: (int(q[c]), float(ms[c])) for c in range(55) if q[c]}
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped entry points (src/integrals/base.h:39-93).  The first
+# argument is the FockEngine that stands in for the shell-pair vector.
+# ---------------------------------------------------------------------------
+def _prepare(eng, nbasis, engine, tol_eri, sym_ops):
+    if sym_ops is not None and len(sym_ops) > 1:
+        raise PfkError(PFK_ERR_UNSUPPORTED, "integral symmetry operations are not supported; pass None")
+    if nbasis != eng.nbasis:
+        raise PfkError(PFK_ERR_INVALID, f"nbasis {nbasis} does not match the engine ({eng.nbasis})")
+    if tol_eri != eng.tol_eri or engine != eng.engine:
+        eng.set_options(tol_eri, engine, eng.precision, eng.fp32_bound)
+
+
+def _compute_2e(eng, nbasis, engine="os", tol_eri=1e-10, sym_ops=None):
+    """Dense nb^4 tensor, row-major (base.h:39-55)."""
+    _prepare(eng, nbasis, engine, tol_eri, sym_ops)
+    return eng.eri_tensor().reshape(-1)
+
+
+def _compute_2e_fock(eng, density, nbasis, engine="os", tol_eri=1e-10, sym_ops=None):
+    """G = J - K/2 (base.h:57-73)."""
+    _prepare(eng, nbasis, engine, tol_eri, sym_ops)
+    return eng.fock_rhf(density)
+
+
+def _compute_2e_fock_uhf(eng, Pa, Pb, nbasis, engine="os", tol_eri=1e-10, sym_ops=None):
+    """(G_alpha, G_beta) (base.h:75-93)."""
+    _prepare(eng, nbasis, engine, tol_eri, sym_ops)
+    return eng.fock_uhf(Pa, Pb)

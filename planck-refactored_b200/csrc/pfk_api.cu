@@ -1,0 +1,738 @@
+// pfk_api.cu -- the C ABI (include/planck_fock.h): context, per-geometry
+// setup, and the per-iteration Fock builds.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/planck_fock.h"
+#include "pfk_internal.h"
+#include "pfk_setup.h"
+
+using namespace pfk;
+
+namespace {
+
+thread_local std::string g_last_error;   // for failures without a context
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count)
+    {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(reinterpret_cast<void **>(&p), sizeof(T) * count);
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct GraphEntry {
+    const void *in;
+    void *out;
+    cudaStream_t stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace
+
+struct pfk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    int nshell = 0, nb = 0;
+    std::vector<int> L, bf_off;
+
+    int npairs = 0;
+    std::vector<PairInfo> pairs;
+    std::vector<int> pair_pc, pair_la, pair_lb;
+    std::vector<PrimPair> prims;
+    DevBuf<PairInfo> d_pairs;
+    DevBuf<PrimPair> d_prims;
+    DevBuf<int> d_pair_la, d_pair_lb;
+
+    std::vector<double> Q;
+    DevBuf<double> d_Q;
+
+    std::vector<int> cls_ids[kPairClasses];
+    DevBuf<int> d_cls_ids[kPairClasses];
+    DevBuf<double> d_cls_q[kPairClasses];
+
+    double tol = 1e-10, fp32_bound = 1e-8;
+    int engine = PFK_ENGINE_OS, precision = PFK_PREC_FP64;
+
+    DevBuf<uint2> d_quart;
+    long long q_off[kQuartetClasses] = {}, q_cnt[kQuartetClasses] = {};
+    long long q32_off[kQuartetClasses] = {}, q32_cnt[kQuartetClasses] = {};
+    ClassLauncher launch[kQuartetClasses] = {};
+    float class_ms[kQuartetClasses] = {};
+
+    DevBuf<double> d_P, d_Pb, d_Pt, d_J, d_K0, d_K1, d_G, d_Gb;
+    std::vector<GraphEntry> graphs;
+
+    pfk_status fail(pfk_status s, const std::string &msg)
+    {
+        err = msg;
+        return s;
+    }
+    pfk_status cuda_fail(const char *what, cudaError_t e)
+    {
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return PFK_ERR_CUDA;
+    }
+};
+
+#define PFK_CK(call)                                                    \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return ctx->cuda_fail(#call, e_);        \
+    } while (0)
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+pfk_status validate(const pfk_basis_desc *b, std::string &why)
+{
+    if (!b || b->nshell <= 0 || !b->L || !b->nprim || !b->center || !b->expo || !b->coef || !b->norm) {
+        why = "basis descriptor is null or empty";
+        return PFK_ERR_INVALID;
+    }
+    long long nb = 0, np = 0;
+    for (int s = 0; s < b->nshell; ++s) {
+        if (b->L[s] < 0) {
+            why = "negative angular momentum";
+            return PFK_ERR_INVALID;
+        }
+        if (b->L[s] > 3) {
+            why = "angular momentum above f (L=3) is not supported";
+            return PFK_ERR_UNSUPPORTED;
+        }
+        if (b->nprim[s] <= 0 || b->nprim[s] > 64) {
+            why = "primitive count per shell must be 1..64";
+            return PFK_ERR_INVALID;
+        }
+        for (int d = 0; d < 3; ++d)
+            if (!std::isfinite(b->center[3 * s + d])) {
+                why = "non-finite shell centre";
+                return PFK_ERR_INVALID;
+            }
+        nb += ncart(b->L[s]);
+        np += b->nprim[s];
+    }
+    for (long long i = 0; i < np; ++i)
+        if (!(b->expo[i] > 0.0) || !std::isfinite(b->expo[i]) || !std::isfinite(b->coef[i]) || !std::isfinite(b->norm[i])) {
+            why = "exponents must be positive and finite; coefficients and norms finite";
+            return PFK_ERR_INVALID;
+        }
+    if (nb >= 65536) {
+        why = "more than 65535 basis functions";
+        return PFK_ERR_UNSUPPORTED;
+    }
+    return PFK_OK;
+}
+
+// Shell pairs a <= b with primitive-pair data (src/base/types.h:631-674),
+// oriented so that L(A) >= L(B).
+void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
+{
+    std::vector<int> poff(b->nshell + 1, 0);
+    for (int s = 0; s < b->nshell; ++s) poff[s + 1] = poff[s] + b->nprim[s];
+    ctx->pairs.clear();
+    ctx->prims.clear();
+    for (int sa = 0; sa < b->nshell; ++sa)
+        for (int sb = sa; sb < b->nshell; ++sb) {
+            const int A = b->L[sa] >= b->L[sb] ? sa : sb;
+            const int B = A == sa ? sb : sa;
+            const double *ca = b->center + 3 * A, *cb = b->center + 3 * B;
+            PairInfo pi{};
+            pi.prim_off = (int)ctx->prims.size();
+            pi.nprim = b->nprim[A] * b->nprim[B];
+            pi.bf_a = ctx->bf_off[A];
+            pi.bf_b = ctx->bf_off[B];
+            pi.ABx = ca[0] - cb[0];
+            pi.ABy = ca[1] - cb[1];
+            pi.ABz = ca[2] - cb[2];
+            const double R2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+            for (int ia = 0; ia < b->nprim[A]; ++ia)
+                for (int ib = 0; ib < b->nprim[B]; ++ib) {
+                    const double alpha = b->expo[poff[A] + ia], beta = b->expo[poff[B] + ib];
+                    const double zeta = alpha + beta, iz = 1.0 / zeta;
+                    PrimPair p{};
+                    p.zeta = zeta;
+                    p.inv_zeta = iz;
+                    p.Px = (alpha * ca[0] + beta * cb[0]) * iz;
+                    p.Py = (alpha * ca[1] + beta * cb[1]) * iz;
+                    p.Pz = (alpha * ca[2] + beta * cb[2]) * iz;
+                    p.PAx = p.Px - ca[0];
+                    p.PAy = p.Py - ca[1];
+                    p.PAz = p.Pz - ca[2];
+                    p.K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) * b->coef[poff[A] + ia] *
+                          b->coef[poff[B] + ib] * b->norm[poff[A] + ia] * b->norm[poff[B] + ib];
+                    ctx->prims.push_back(p);
+                }
+            ctx->pairs.push_back(pi);
+            ctx->pair_pc.push_back(pair_class(b->L[A], b->L[B]));
+            ctx->pair_la.push_back(b->L[A]);
+            ctx->pair_lb.push_back(b->L[B]);
+        }
+    ctx->npairs = (int)ctx->pairs.size();
+}
+
+pfk_status upload_pairs(pfk_ctx *ctx)
+{
+    PFK_CK(ctx->d_pairs.alloc(ctx->npairs));
+    PFK_CK(cudaMemcpyAsync(ctx->d_pairs.p, ctx->pairs.data(), sizeof(PairInfo) * ctx->npairs, cudaMemcpyHostToDevice,
+                           ctx->stream));
+    return PFK_OK;
+}
+
+// Screened shell-quartet lists for the current tol / FP32 bound.
+pfk_status build_lists(pfk_ctx *ctx)
+{
+    const double bound = ctx->precision == PFK_PREC_MIXED ? ctx->fp32_bound : 0.0;
+    int maxn = 1;
+    for (int x = 0; x < kPairClasses; ++x) maxn = std::max(maxn, (int)ctx->cls_ids[x].size());
+    DevBuf<long long> cnt_hi, cnt_lo, off_hi, off_lo;
+    PFK_CK(cnt_hi.alloc(maxn));
+    PFK_CK(cnt_lo.alloc(maxn));
+    PFK_CK(off_hi.alloc(maxn));
+    PFK_CK(off_lo.alloc(maxn));
+    size_t tmp_bytes = 0;
+    PFK_CK(exclusive_scan(cnt_hi.p, off_hi.p, maxn, nullptr, tmp_bytes, ctx->stream));
+    DevBuf<char> tmp;
+    PFK_CK(tmp.alloc(tmp_bytes + 16));
+
+    // pass 1: counts
+    long long total = 0;
+    for (int x = 0; x < kPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            const int cls = quartet_class(x, y);
+            const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
+            ctx->q_cnt[cls] = ctx->q32_cnt[cls] = 0;
+            if (nX == 0 || nY == 0) continue;
+            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
+                                  cnt_lo.p, ctx->stream));
+            size_t tb = tmp_bytes;
+            PFK_CK(exclusive_scan(cnt_hi.p, off_hi.p, nX, tmp.p, tb, ctx->stream));
+            tb = tmp_bytes;
+            PFK_CK(exclusive_scan(cnt_lo.p, off_lo.p, nX, tmp.p, tb, ctx->stream));
+            long long h[4];
+            PFK_CK(cudaMemcpyAsync(&h[0], off_hi.p + nX - 1, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(&h[1], cnt_hi.p + nX - 1, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(&h[2], off_lo.p + nX - 1, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(&h[3], cnt_lo.p + nX - 1, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaStreamSynchronize(ctx->stream));
+            ctx->q_cnt[cls] = h[0] + h[1];
+            ctx->q32_cnt[cls] = h[2] + h[3];
+            total += ctx->q_cnt[cls] + ctx->q32_cnt[cls];
+        }
+    long long pos = 0;
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        ctx->q_off[c] = pos;
+        pos += ctx->q_cnt[c];
+        ctx->q32_off[c] = pos;
+        pos += ctx->q32_cnt[c];
+    }
+    PFK_CK(ctx->d_quart.alloc((size_t)std::max(total, 1LL)));
+    // pass 2: fill
+    for (int x = 0; x < kPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            const int cls = quartet_class(x, y);
+            const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
+            if (nX == 0 || nY == 0 || ctx->q_cnt[cls] + ctx->q32_cnt[cls] == 0) continue;
+            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
+                                  cnt_lo.p, ctx->stream));
+            size_t tb = tmp_bytes;
+            PFK_CK(exclusive_scan(cnt_hi.p, off_hi.p, nX, tmp.p, tb, ctx->stream));
+            tb = tmp_bytes;
+            PFK_CK(exclusive_scan(cnt_lo.p, off_lo.p, nX, tmp.p, tb, ctx->stream));
+            PFK_CK(fill_quartets(ctx->d_cls_ids[x].p, nX, ctx->d_cls_ids[y].p, x == y, off_hi.p, cnt_hi.p, off_lo.p,
+                                 cnt_lo.p, ctx->d_quart.p + ctx->q_off[cls], ctx->d_quart.p + ctx->q32_off[cls],
+                                 ctx->stream));
+        }
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    for (auto &g : ctx->graphs) {   // captured builds refer to the old lists
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->graphs.clear();
+    return PFK_OK;
+}
+
+pfk_status schwarz_and_sort(pfk_ctx *ctx)
+{
+    const int nb = ctx->nb;
+    PFK_CK(ctx->d_Q.alloc((size_t)nb * nb));
+    PFK_CK(cudaMemsetAsync(ctx->d_Q.p, 0, sizeof(double) * nb * nb, ctx->stream));
+    std::vector<int> ids[kPairClasses];
+    for (int p = 0; p < ctx->npairs; ++p) ids[ctx->pair_pc[p]].push_back(p);
+    DevBuf<int> d_ids[kPairClasses];
+    for (int x = 0; x < kPairClasses; ++x) {
+        if (ids[x].empty()) continue;
+        PFK_CK(d_ids[x].alloc(ids[x].size()));
+        PFK_CK(cudaMemcpyAsync(d_ids[x].p, ids[x].data(), sizeof(int) * ids[x].size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
+        launch_schwarz(x, d_ids[x].p, (int)ids[x].size(), ctx->d_pairs.p, ctx->d_prims.p, ctx->d_Q.p, nb, ctx->stream);
+        PFK_CK(cudaGetLastError());
+    }
+    ctx->Q.assign((size_t)nb * nb, 0.0);
+    PFK_CK(cudaMemcpyAsync(ctx->Q.data(), ctx->d_Q.p, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    for (int x = 0; x < kPairClasses; ++x) ids[x].clear();
+    // per-pair bound over components
+    for (int p = 0; p < ctx->npairs; ++p) {
+        PairInfo &pi = ctx->pairs[p];
+        const int na = ncart(ctx->pair_la[p]), nbb = ncart(ctx->pair_lb[p]);
+        double qmax = 0.0, qmin = INFINITY;
+        for (int a = 0; a < na; ++a)
+            for (int c = 0; c < nbb; ++c) {
+                const double q = ctx->Q[(size_t)(pi.bf_a + a) * nb + pi.bf_b + c];
+                qmax = std::max(qmax, q);
+                qmin = std::min(qmin, q);
+            }
+        pi.qmax = qmax;
+        pi.qmin = qmin;
+    }
+    pfk_status s = upload_pairs(ctx);
+    if (s != PFK_OK) return s;
+    // per-class lists sorted by qmax, descending (ties by pair index)
+    for (int p = 0; p < ctx->npairs; ++p) ids[ctx->pair_pc[p]].push_back(p);
+    for (int x = 0; x < kPairClasses; ++x) {
+        auto &v = ids[x];
+        std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return ctx->pairs[a].qmax > ctx->pairs[b].qmax; });
+        ctx->cls_ids[x] = v;
+        std::vector<double> q(v.size());
+        for (size_t i = 0; i < v.size(); ++i) q[i] = ctx->pairs[v[i]].qmax;
+        if (v.empty()) continue;
+        PFK_CK(ctx->d_cls_ids[x].alloc(v.size()));
+        PFK_CK(ctx->d_cls_q[x].alloc(v.size()));
+        PFK_CK(cudaMemcpyAsync(ctx->d_cls_ids[x].p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+        PFK_CK(cudaMemcpyAsync(ctx->d_cls_q[x].p, q.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+        PFK_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return PFK_OK;
+}
+
+// Launch every class kernel over the screened lists.  Jacc/K accumulators are
+// zeroed first.  eri_out selects the dense-tensor mode.
+pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const double *Pk1, int nk, double *Jacc,
+                       double *K0, double *K1, double *eri_out, cudaStream_t st, bool timed)
+{
+    const size_t nb2 = (size_t)ctx->nb * ctx->nb;
+    if (!eri_out) {
+        PFK_CK(cudaMemsetAsync(Jacc, 0, sizeof(double) * nb2, st));
+        if (K0) PFK_CK(cudaMemsetAsync(K0, 0, sizeof(double) * nb2, st));
+        if (K1) PFK_CK(cudaMemsetAsync(K1, 0, sizeof(double) * nb2, st));
+    }
+    JKArgs a{};
+    a.pairs = ctx->d_pairs.p;
+    a.prims = ctx->d_prims.p;
+    a.Qao = ctx->d_Q.p;
+    a.Pj = Pj;
+    a.Pk0 = Pk0;
+    a.Pk1 = Pk1;
+    a.Jacc = Jacc;
+    a.Kacc0 = K0;
+    a.Kacc1 = K1;
+    a.eri_out = eri_out;
+    a.tol = ctx->tol;
+    a.nb = ctx->nb;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (timed) {
+        PFK_CK(cudaEventCreate(&ev[0]));
+        PFK_CK(cudaEventCreate(&ev[1]));
+    }
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        const long long n = ctx->q_cnt[c] + ctx->q32_cnt[c];
+        if (n == 0) continue;
+        if (timed) PFK_CK(cudaEventRecord(ev[0], st));
+        if (ctx->q_cnt[c]) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], ctx->q_cnt[c], a, nk, st);
+        if (ctx->q32_cnt[c]) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], ctx->q32_cnt[c], a, nk, st);
+        PFK_CK(cudaGetLastError());
+        if (timed) {
+            PFK_CK(cudaEventRecord(ev[1], st));
+            PFK_CK(cudaEventSynchronize(ev[1]));
+            float ms = 0.f;
+            PFK_CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            ctx->class_ms[c] = ms;
+        }
+    }
+    if (timed) {
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
+    return PFK_OK;
+}
+
+pfk_status rhf_sequence(pfk_ctx *ctx, const double *dP, double *dG, cudaStream_t st)
+{
+    pfk_status s = run_classes(ctx, dP, dP, nullptr, 1, ctx->d_J.p, ctx->d_K0.p, nullptr, nullptr, st, false);
+    if (s != PFK_OK) return s;
+    PFK_CK(combine(ctx->d_J.p, ctx->d_K0.p, 1.0, -0.5, dG, ctx->nb, st));
+    return PFK_OK;
+}
+
+pfk_status ensure_work(pfk_ctx *ctx)
+{
+    const size_t nb2 = (size_t)ctx->nb * ctx->nb;
+    if (ctx->d_J.p) return PFK_OK;
+    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
+        PFK_CK(b->alloc(nb2));
+    return PFK_OK;
+}
+
+pfk_status check_symmetric(pfk_ctx *ctx, const double *P)
+{
+    const int nb = ctx->nb;
+    double amax = 0.0, dmax = 0.0;
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) {
+            amax = std::max(amax, std::fabs(P[(size_t)i * nb + j]));
+            if (j > i) dmax = std::max(dmax, std::fabs(P[(size_t)i * nb + j] - P[(size_t)j * nb + i]));
+        }
+    if (!(dmax <= 1e-10 * std::max(1.0, amax)))
+        return ctx->fail(PFK_ERR_INVALID, "density matrix is not symmetric (or not finite)");
+    return PFK_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
+{
+    if (!out) {
+        g_last_error = "pfk_create: out is null";
+        return PFK_ERR_INVALID;
+    }
+    *out = nullptr;
+    std::string why;
+    pfk_status vs = validate(basis, why);
+    if (vs != PFK_OK) {
+        g_last_error = "pfk_create: " + why;
+        return vs;
+    }
+    pfk_ctx *ctx = nullptr;
+    try {
+        ctx = new pfk_ctx();
+    } catch (const std::bad_alloc &) {
+        g_last_error = "pfk_create: host allocation failed";
+        return PFK_ERR_NOMEM;
+    }
+    auto bail = [&](pfk_status s) {
+        g_last_error = ctx->err;
+        pfk_destroy(ctx);
+        return s;
+    };
+    try {
+        ctx->device = device;
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaSetDevice", e));
+        e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaStreamCreate", e));
+        ctx->nshell = basis->nshell;
+        ctx->L.assign(basis->L, basis->L + basis->nshell);
+        ctx->bf_off.resize(basis->nshell);
+        int nb = 0;
+        for (int s = 0; s < basis->nshell; ++s) {
+            ctx->bf_off[s] = nb;
+            nb += ncart(basis->L[s]);
+        }
+        ctx->nb = nb;
+        build_pairs(ctx, basis);
+        e = ctx->d_prims.alloc(ctx->prims.size());
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaMalloc(prims)", e));
+        e = cudaMemcpyAsync(ctx->d_prims.p, ctx->prims.data(), sizeof(PrimPair) * ctx->prims.size(),
+                            cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaMemcpy(prims)", e));
+        e = ctx->d_pair_la.alloc(ctx->npairs);
+        if (e == cudaSuccess) e = ctx->d_pair_lb.alloc(ctx->npairs);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ctx->d_pair_la.p, ctx->pair_la.data(), sizeof(int) * ctx->npairs, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ctx->d_pair_lb.p, ctx->pair_lb.data(), sizeof(int) * ctx->npairs, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("pair tables", e));
+        pfk_status s = upload_pairs(ctx);
+        if (s != PFK_OK) return bail(s);
+        register_bra_class_0(ctx->launch);
+        register_bra_class_1(ctx->launch);
+        register_bra_class_2(ctx->launch);
+        register_bra_class_3(ctx->launch);
+        register_bra_class_4(ctx->launch);
+        register_bra_class_5(ctx->launch);
+        register_bra_class_6(ctx->launch);
+        register_bra_class_7(ctx->launch);
+        register_bra_class_8(ctx->launch);
+        register_bra_class_9(ctx->launch);
+        JKArgs none{};
+        for (int c = 0; c < kQuartetClasses; ++c) ctx->launch[c](nullptr, -1, none, 1, ctx->stream);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("kernel configuration", e));
+        s = schwarz_and_sort(ctx);
+        if (s != PFK_OK) return bail(s);
+        s = build_lists(ctx);
+        if (s != PFK_OK) return bail(s);
+        s = ensure_work(ctx);
+        if (s != PFK_OK) return bail(s);
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host allocation failed";
+        return bail(PFK_ERR_NOMEM);
+    }
+    *out = ctx;
+    return PFK_OK;
+}
+
+pfk_status pfk_destroy(pfk_ctx *ctx)
+{
+    if (!ctx) return PFK_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &g : ctx->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->d_pairs.release();
+    ctx->d_prims.release();
+    ctx->d_pair_la.release();
+    ctx->d_pair_lb.release();
+    ctx->d_Q.release();
+    for (int x = 0; x < kPairClasses; ++x) {
+        ctx->d_cls_ids[x].release();
+        ctx->d_cls_q[x].release();
+    }
+    ctx->d_quart.release();
+    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
+        b->release();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PFK_OK;
+}
+
+int pfk_nbasis(const pfk_ctx *ctx) { return ctx ? ctx->nb : 0; }
+
+const char *pfk_last_error(const pfk_ctx *ctx) { return ctx ? ctx->err.c_str() : g_last_error.c_str(); }
+
+pfk_status pfk_set_options(pfk_ctx *ctx, double tol_eri, int engine, int precision, double fp32_bound)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!(tol_eri >= 0.0) || !std::isfinite(tol_eri)) return ctx->fail(PFK_ERR_INVALID, "tol_eri must be finite and >= 0");
+    if (engine < PFK_ENGINE_OS || engine > PFK_ENGINE_AUTO) return ctx->fail(PFK_ERR_INVALID, "unknown engine");
+    if (precision != PFK_PREC_FP64 && precision != PFK_PREC_MIXED) return ctx->fail(PFK_ERR_INVALID, "unknown precision");
+    if (precision == PFK_PREC_MIXED && !(fp32_bound > 0.0 && std::isfinite(fp32_bound)))
+        return ctx->fail(PFK_ERR_INVALID, "fp32_bound must be positive");
+    cudaSetDevice(ctx->device);
+    const bool rebuild = tol_eri != ctx->tol || precision != ctx->precision ||
+                         (precision == PFK_PREC_MIXED && fp32_bound != ctx->fp32_bound);
+    ctx->tol = tol_eri;
+    ctx->engine = engine;
+    ctx->precision = precision;
+    if (precision == PFK_PREC_MIXED) ctx->fp32_bound = fp32_bound;
+    return rebuild ? build_lists(ctx) : PFK_OK;
+}
+
+pfk_status pfk_schwarz(pfk_ctx *ctx, double *Q)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!Q) return ctx->fail(PFK_ERR_INVALID, "Q is null");
+    std::memcpy(Q, ctx->Q.data(), sizeof(double) * ctx->Q.size());
+    return PFK_OK;
+}
+
+static pfk_status run_census(pfk_ctx *ctx, long long *n_ao, uint64_t *digest, long long *n_shell, int *out, long long cap)
+{
+    cudaSetDevice(ctx->device);
+    DevBuf<unsigned long long> cnt;
+    PFK_CK(cnt.alloc(3));
+    PFK_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * 3, ctx->stream));
+    DevBuf<int> d_out;
+    if (out && cap > 0) PFK_CK(d_out.alloc((size_t)cap * 4));
+    long long nsh = 0;
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        const long long n = ctx->q_cnt[c] + ctx->q32_cnt[c];
+        nsh += n;
+        if (n == 0) continue;
+        PFK_CK(census(ctx->d_quart.p + ctx->q_off[c], n, ctx->d_pairs.p, ctx->d_pair_la.p, ctx->d_pair_lb.p,
+                      ctx->d_Q.p, ctx->nb, ctx->tol, cnt.p, d_out.p, cap, ctx->stream));
+    }
+    unsigned long long h[3];
+    PFK_CK(cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    if (out && cap > 0) {
+        const long long m = std::min<long long>(cap, (long long)h[2]);
+        PFK_CK(cudaMemcpy(out, d_out.p, sizeof(int) * 4 * m, cudaMemcpyDeviceToHost));
+    }
+    if (n_ao) *n_ao = (long long)h[0];
+    if (digest) *digest = h[1];
+    if (n_shell) *n_shell = nsh;
+    return PFK_OK;
+}
+
+pfk_status pfk_quartet_count(pfk_ctx *ctx, long long *n_ao_quartets, uint64_t *digest, long long *n_shell_quartets)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    return run_census(ctx, n_ao_quartets, digest, n_shell_quartets, nullptr, 0);
+}
+
+pfk_status pfk_quartet_list(pfk_ctx *ctx, int *out, long long cap, long long *n)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!out || cap < 0) return ctx->fail(PFK_ERR_INVALID, "output buffer is null");
+    return run_census(ctx, n, nullptr, nullptr, out, cap);
+}
+
+// Captured-graph replay of the RHF build for a (dP, dG, stream) triple.
+static pfk_status rhf_graph(pfk_ctx *ctx, const double *dP, double *dG, cudaStream_t st)
+{
+    GraphEntry *ge = nullptr;
+    for (auto &g : ctx->graphs)
+        if (g.in == dP && g.out == dG && g.stream == st) ge = &g;
+    if (!ge) {
+        GraphEntry g{dP, dG, st};
+        PFK_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        pfk_status s = rhf_sequence(ctx, dP, dG, st);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &graph);
+        if (s != PFK_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return s;
+        }
+        if (e != cudaSuccess) return ctx->cuda_fail("cudaStreamEndCapture", e);
+        g.graph = graph;
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return ctx->cuda_fail("cudaGraphInstantiate", e);
+        }
+        ctx->graphs.push_back(g);
+        ge = &ctx->graphs.back();
+    }
+    PFK_CK(cudaGraphLaunch(ge->exec, st));
+    return PFK_OK;
+}
+
+pfk_status pfk_fock_rhf(pfk_ctx *ctx, const double *P, double *G)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!P || !G) return ctx->fail(PFK_ERR_INVALID, "null matrix");
+    pfk_status s = check_symmetric(ctx, P);
+    if (s != PFK_OK) return s;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(double) * ctx->nb * ctx->nb;
+    PFK_CK(cudaMemcpyAsync(ctx->d_P.p, P, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    s = rhf_graph(ctx, ctx->d_P.p, ctx->d_G.p, ctx->stream);
+    if (s != PFK_OK) return s;
+    PFK_CK(cudaMemcpyAsync(G, ctx->d_G.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    return PFK_OK;
+}
+
+pfk_status pfk_fock_rhf_device(pfk_ctx *ctx, const double *dP, double *dG, void *stream)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!dP || !dG) return ctx->fail(PFK_ERR_INVALID, "null matrix");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    return rhf_graph(ctx, dP, dG, st);
+}
+
+pfk_status pfk_fock_uhf(pfk_ctx *ctx, const double *Pa, const double *Pb, double *Ga, double *Gb)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!Pa || !Pb || !Ga || !Gb) return ctx->fail(PFK_ERR_INVALID, "null matrix");
+    pfk_status s = check_symmetric(ctx, Pa);
+    if (s == PFK_OK) s = check_symmetric(ctx, Pb);
+    if (s != PFK_OK) return s;
+    cudaSetDevice(ctx->device);
+    const size_t nb2 = (size_t)ctx->nb * ctx->nb, bytes = sizeof(double) * nb2;
+    cudaStream_t st = ctx->stream;
+    PFK_CK(cudaMemcpyAsync(ctx->d_P.p, Pa, bytes, cudaMemcpyHostToDevice, st));
+    PFK_CK(cudaMemcpyAsync(ctx->d_Pb.p, Pb, bytes, cudaMemcpyHostToDevice, st));
+    PFK_CK(add(ctx->d_P.p, ctx->d_Pb.p, ctx->d_Pt.p, (long long)nb2, st));
+    s = run_classes(ctx, ctx->d_Pt.p, ctx->d_P.p, ctx->d_Pb.p, 2, ctx->d_J.p, ctx->d_K0.p, ctx->d_K1.p, nullptr, st, false);
+    if (s != PFK_OK) return s;
+    PFK_CK(combine(ctx->d_J.p, ctx->d_K0.p, 1.0, -1.0, ctx->d_G.p, ctx->nb, st));
+    PFK_CK(combine(ctx->d_J.p, ctx->d_K1.p, 1.0, -1.0, ctx->d_Gb.p, ctx->nb, st));
+    PFK_CK(cudaMemcpyAsync(Ga, ctx->d_G.p, bytes, cudaMemcpyDeviceToHost, st));
+    PFK_CK(cudaMemcpyAsync(Gb, ctx->d_Gb.p, bytes, cudaMemcpyDeviceToHost, st));
+    PFK_CK(cudaStreamSynchronize(st));
+    return PFK_OK;
+}
+
+pfk_status pfk_jk(pfk_ctx *ctx, const double *P, const double *Pk, double *J, double *K, double k_scale)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!P || !J) return ctx->fail(PFK_ERR_INVALID, "null matrix");
+    if (!Pk) Pk = P;
+    pfk_status s = check_symmetric(ctx, P);
+    if (s == PFK_OK && Pk != P) s = check_symmetric(ctx, Pk);
+    if (s != PFK_OK) return s;
+    cudaSetDevice(ctx->device);
+    const size_t nb2 = (size_t)ctx->nb * ctx->nb, bytes = sizeof(double) * nb2;
+    cudaStream_t st = ctx->stream;
+    PFK_CK(cudaMemcpyAsync(ctx->d_P.p, P, bytes, cudaMemcpyHostToDevice, st));
+    const double *dPk = ctx->d_P.p;
+    if (Pk != P) {
+        PFK_CK(cudaMemcpyAsync(ctx->d_Pb.p, Pk, bytes, cudaMemcpyHostToDevice, st));
+        dPk = ctx->d_Pb.p;
+    }
+    s = run_classes(ctx, ctx->d_P.p, dPk, nullptr, 1, ctx->d_J.p, K ? ctx->d_K0.p : nullptr, nullptr, nullptr, st, false);
+    if (s != PFK_OK) return s;
+    PFK_CK(combine(ctx->d_J.p, nullptr, 1.0, 0.0, ctx->d_G.p, ctx->nb, st));
+    PFK_CK(cudaMemcpyAsync(J, ctx->d_G.p, bytes, cudaMemcpyDeviceToHost, st));
+    if (K) {
+        PFK_CK(combine(nullptr, ctx->d_K0.p, 0.0, k_scale, ctx->d_Gb.p, ctx->nb, st));
+        PFK_CK(cudaMemcpyAsync(K, ctx->d_Gb.p, bytes, cudaMemcpyDeviceToHost, st));
+    }
+    PFK_CK(cudaStreamSynchronize(st));
+    return PFK_OK;
+}
+
+pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!eri) return ctx->fail(PFK_ERR_INVALID, "eri is null");
+    if (ctx->nb > 180) return ctx->fail(PFK_ERR_UNSUPPORTED, "dense tensor limited to 180 basis functions (8.4 GB)");
+    cudaSetDevice(ctx->device);
+    const size_t n4 = (size_t)ctx->nb * ctx->nb * ctx->nb * ctx->nb;
+    DevBuf<double> d;
+    PFK_CK(d.alloc(n4));
+    PFK_CK(cudaMemsetAsync(d.p, 0, sizeof(double) * n4, ctx->stream));
+    pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, d.p, ctx->stream, false);
+    if (s != PFK_OK) return s;
+    PFK_CK(cudaMemcpyAsync(eri, d.p, sizeof(double) * n4, cudaMemcpyDeviceToHost, ctx->stream));
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    return PFK_OK;
+}
+
+pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, double *ms55)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    if (ms55) {
+        pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, ctx->d_K0.p, nullptr, nullptr,
+                                   ctx->stream, true);
+        if (s != PFK_OK) return s;
+        for (int c = 0; c < kQuartetClasses; ++c) ms55[c] = ctx->class_ms[c];
+    }
+    if (quartets55)
+        for (int c = 0; c < kQuartetClasses; ++c) quartets55[c] = ctx->q_cnt[c] + ctx->q32_cnt[c];
+    return PFK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,267 @@
+// pfk_device.cuh -- device-side building blocks of the Fock engine (sm_100a).
+//
+// Integral method: Rys quadrature (the reference's RysQuad path,
+// src/integrals/rys.cpp:250-485), reorganised for the GPU:
+//   * one shell quartet (all Cartesian components) per thread or per team,
+//     instead of one Cartesian component quartet per call;
+//   * roots/weights from piecewise Chebyshev tables generated offline in
+//     80-digit arithmetic (gen_rys_table.py) instead of a per-primitive
+//     long-double moment/eigensolver construction (rys_roots.cpp:88-235);
+//   * the A->B and C->D transfer (rys.cpp:293-363) applied per Cartesian
+//     axis to the 2D integrals of each root, so the 6D product is formed
+//     only for the output components;
+//   * J/K digestion fused into the integral kernel (os.cpp:1512-1520 does it
+//     as a separate O(nb^4) pass over a stored tensor).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pfk {
+
+// ---------------------------------------------------------------------------
+// Shapes
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+__host__ __device__ constexpr int cart_block(int i)
+{
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= i) ++n;
+    return n;
+}
+// Cartesian component i of a shell of angular momentum L, in the reference's
+// order (lx descending, then ly descending; src/basis/basis.cpp:20-37).
+__host__ __device__ constexpr int cart_lx(int L, int i) { return L - cart_block(i); }
+__host__ __device__ constexpr int cart_lz(int L, int i)
+{
+    return i - cart_block(i) * (cart_block(i) + 1) / 2;
+}
+__host__ __device__ constexpr int cart_ly(int L, int i) { return L - cart_lx(L, i) - cart_lz(L, i); }
+__host__ __device__ constexpr int dfact(int n) { return n <= 0 ? 1 : n * dfact(n - 2); }
+// 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!) (src/basis/gaussian.cpp:283-296); the
+// double factorials for L <= 3 are 1, 1, 3, 15, so the square roots below are
+// of small integers.
+__host__ __device__ constexpr double inv_sqrt_small(int d)
+{
+    return d == 1 ? 1.0 : d == 3 ? 0.57735026918962576451 : d == 9 ? 1.0 / 3.0
+         : d == 15 ? 0.25819888974716112568 : 0.0;
+}
+__host__ __device__ constexpr double cart_norm(int L, int i)
+{
+    return inv_sqrt_small(dfact(2 * cart_lx(L, i) - 1) * dfact(2 * cart_ly(L, i) - 1) *
+                          dfact(2 * cart_lz(L, i) - 1));
+}
+
+// ---------------------------------------------------------------------------
+// Data layout in HBM
+// ---------------------------------------------------------------------------
+// One primitive pair of an (oriented) shell pair: Gaussian product data.
+// K = (pi/zeta)^1.5 exp(-alpha beta |AB|^2 / zeta) c_a c_b N_a N_b
+// (src/base/types.h:631-674 without the component norms, which are applied
+// per Cartesian component after contraction).
+struct __align__(16) PrimPair {
+    double zeta, inv_zeta;
+    double Px, Py, Pz;
+    double PAx, PAy, PAz;   // P - A (A = first centre of the oriented pair)
+    double K, pad;
+};
+
+// Shell pair a <= b (shell order), oriented so that L(A) >= L(B).
+struct __align__(16) PairInfo {
+    int prim_off, nprim;     // range in the PrimPair array
+    int bf_a, bf_b;          // first basis function of A and of B
+    double ABx, ABy, ABz;    // A - B
+    double qmax, qmin;       // max / min of Q(i,j) over the pair's components
+};
+
+struct JKArgs {
+    const PairInfo *__restrict__ pairs;
+    const PrimPair *__restrict__ prims;
+    const double *__restrict__ Qao;    // nb x nb Schwarz table
+    const double *__restrict__ Pj;     // density for J
+    const double *__restrict__ Pk0;    // densities for K (Pk1 used when NK == 2)
+    const double *__restrict__ Pk1;
+    double *Jacc;                       // nb x nb accumulators (unsymmetrised)
+    double *Kacc0;
+    double *Kacc1;
+    double *eri_out;                    // dense tensor mode (nb^4) when non-null
+    double tol;
+    int nb;
+};
+
+// ---------------------------------------------------------------------------
+// Rys roots and weights
+// ---------------------------------------------------------------------------
+#define PFK_RYS_CONST_STORAGE static __constant__ const
+#define PFK_RYS_TABLE_STORAGE static __device__ const
+#include "rys_table_data.inc"
+
+__device__ __forceinline__ double clenshaw15(const double *__restrict__ c, double x)
+{
+    double b1 = 0.0, b2 = 0.0;
+    const double x2 = 2.0 * x;
+#pragma unroll
+    for (int k = PFK_RYS_DEG; k >= 1; --k) {
+        const double t = fma(x2, b1, __ldg(c + k) - b2);
+        b2 = b1;
+        b1 = t;
+    }
+    return fma(x, b1, __ldg(c) - b2);
+}
+
+// All NR roots u_r = t_r^2 and weights of the measure exp(-T u) u^-1/2 / 2 du.
+template <int NR>
+__device__ __forceinline__ void rys_roots(double T, double *u, double *w)
+{
+    if (T < kRysTmax[NR]) {
+        const int iv = (int)(T * (1.0 / PFK_RYS_H));
+        const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
+        const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            u[r] = clenshaw15(base + r * (PFK_RYS_DEG + 1), x);
+            w[r] = clenshaw15(base + (NR + r) * (PFK_RYS_DEG + 1), x);
+        }
+    } else {
+        const double iT = 1.0 / T;
+        const double isT = sqrt(iT);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            u[r] = kRysAsymU[NR][r] * iT;
+            w[r] = kRysAsymW[NR][r] * isT;
+        }
+    }
+}
+
+template <int NR>
+__device__ __forceinline__ void rys_root_one(double T, int r, double &u, double &w)
+{
+    if (T < kRysTmax[NR]) {
+        const int iv = (int)(T * (1.0 / PFK_RYS_H));
+        const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
+        const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
+        u = clenshaw15(base + r * (PFK_RYS_DEG + 1), x);
+        w = clenshaw15(base + (NR + r) * (PFK_RYS_DEG + 1), x);
+    } else {
+        const double iT = 1.0 / T;
+        u = kRysAsymU[NR][r] * iT;
+        w = kRysAsymW[NR][r] * sqrt(iT);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-axis 2D integrals of one root (rys.cpp:250-280 recurrence), then the
+// A->B and C->D transfers on that axis (rys.cpp:293-363 applied per axis):
+// out[((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d] = I_axis(a, b, c, d).
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void axis_table(R C00, R D00, R B00, R B10, R B01, R AB, R CD, R scale,
+                                           R *__restrict__ out)
+{
+    constexpr int E = LA + LB, F = LC + LD;
+    R I[E + 1][F + 1];
+    I[0][0] = scale;
+    if constexpr (E > 0) I[1][0] = C00 * scale;
+#pragma unroll
+    for (int a = 1; a < E; ++a) I[a + 1][0] = C00 * I[a][0] + R(a) * B10 * I[a - 1][0];
+#pragma unroll
+    for (int c = 0; c < F; ++c) {
+        I[0][c + 1] = D00 * I[0][c];
+        if (c > 0) I[0][c + 1] += R(c) * B01 * I[0][c - 1];
+#pragma unroll
+        for (int a = 1; a <= E; ++a) {
+            R v = D00 * I[a][c] + R(a) * B00 * I[a - 1][c];
+            if (c > 0) v += R(c) * B01 * I[a][c - 1];
+            I[a][c + 1] = v;
+        }
+    }
+    // A -> B: G[a][b][c] with G(a, b+1) = G(a+1, b) + AB G(a, b)
+    R G[E + 1][LB + 1][F + 1];
+#pragma unroll
+    for (int a = 0; a <= E; ++a)
+#pragma unroll
+        for (int c = 0; c <= F; ++c) G[a][0][c] = I[a][c];
+#pragma unroll
+    for (int b = 0; b < LB; ++b)
+#pragma unroll
+        for (int a = 0; a < E - b; ++a)
+#pragma unroll
+            for (int c = 0; c <= F; ++c) G[a][b + 1][c] = G[a + 1][b][c] + AB * G[a][b][c];
+    // C -> D on the (a <= LA, b <= LB) slice
+#pragma unroll
+    for (int a = 0; a <= LA; ++a)
+#pragma unroll
+        for (int b = 0; b <= LB; ++b) {
+            R H[F + 1][LD + 1];
+#pragma unroll
+            for (int c = 0; c <= F; ++c) H[c][0] = G[a][b][c];
+#pragma unroll
+            for (int d = 0; d < LD; ++d)
+#pragma unroll
+                for (int c = 0; c < F - d; ++c) H[c][d + 1] = H[c + 1][d] + CD * H[c][d];
+#pragma unroll
+            for (int c = 0; c <= LC; ++c)
+#pragma unroll
+                for (int d = 0; d <= LD; ++d)
+                    out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = H[c][d];
+        }
+}
+
+// Per-primitive-quartet scalars shared by all roots.
+struct QuartetScalars {
+    double T, pref, rdelta, rho;
+    double zinv, einv;
+    double WPx, WPy, WPz, WQx, WQy, WQz;
+};
+
+__device__ __forceinline__ QuartetScalars quartet_scalars(const PrimPair &p, const PrimPair &q)
+{
+    QuartetScalars s;
+    const double delta = p.zeta + q.zeta;
+    s.rdelta = 1.0 / delta;
+    s.rho = p.zeta * q.zeta * s.rdelta;
+    const double PQx = p.Px - q.Px, PQy = p.Py - q.Py, PQz = p.Pz - q.Pz;
+    s.T = s.rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+    // 2 sqrt(rho / pi) K_ab K_cd  (rys.cpp:415)
+    s.pref = 1.1283791670955125739 * sqrt(s.rho) * p.K * q.K;
+    s.zinv = p.inv_zeta;
+    s.einv = q.inv_zeta;
+    const double fp = -q.zeta * s.rdelta, fq = p.zeta * s.rdelta;  // W-P = fp PQ, W-Q = fq PQ
+    s.WPx = fp * PQx; s.WPy = fp * PQy; s.WPz = fp * PQz;
+    s.WQx = fq * PQx; s.WQy = fq * PQy; s.WQz = fq * PQz;
+    return s;
+}
+
+__device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, int i)
+{
+    const double2 *v = reinterpret_cast<const double2 *>(a + i);
+    const double2 x0 = __ldg(v), x1 = __ldg(v + 1), x2 = __ldg(v + 2), x3 = __ldg(v + 3), x4 = __ldg(v + 4);
+    PrimPair p;
+    p.zeta = x0.x; p.inv_zeta = x0.y; p.Px = x1.x; p.Py = x1.y; p.Pz = x2.x;
+    p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.K = x4.x; p.pad = 0.0;
+    return p;
+}
+
+// Contribution of one canonical AO quartet to the J/K accumulators:
+// Jacc(i,j) += s v Pj(k,l), Jacc(k,l) += s v Pj(i,j),
+// Kacc(i,k) += s v Pk(j,l), Kacc(j,k) += s v Pk(i,l),
+// Kacc(i,l) += s v Pk(j,k), Kacc(j,l) += s v Pk(i,k);
+// J = 2 (Jacc + Jacc^T), K = Kacc + Kacc^T.  This is the sum over the
+// distinct members of the 8-fold permutation orbit that the reference
+// writes into its tensor (os.cpp:137-163) and then contracts
+// (os.cpp:1514-1520), with s = 1/|stabiliser| removing the duplicates.
+
+// 8-fold scatter of one AO quartet into a dense tensor (os.cpp:137-163).
+__device__ __forceinline__ void scatter8(double *eri, int nb, int i, int j, int k, int l, double v)
+{
+    const size_t n = nb, n2 = n * n, n3 = n2 * n;
+    eri[i * n3 + j * n2 + k * n + l] = v;
+    eri[j * n3 + i * n2 + k * n + l] = v;
+    eri[i * n3 + j * n2 + l * n + k] = v;
+    eri[j * n3 + i * n2 + l * n + k] = v;
+    eri[k * n3 + l * n2 + i * n + j] = v;
+    eri[l * n3 + k * n2 + i * n + j] = v;
+    eri[k * n3 + l * n2 + j * n + i] = v;
+    eri[l * n3 + k * n2 + j * n + i] = v;
+}
+
+}  // namespace pfk

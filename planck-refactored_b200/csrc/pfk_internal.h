@@ -1,0 +1,33 @@
+// pfk_internal.h -- shared host-side declarations of the Fock engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pfk_device.cuh"
+
+namespace pfk {
+
+// Ten shell-pair classes (LA >= LB) in order ss, ps, pp, ds, dp, dd, fs, fp, fd, ff.
+constexpr int kPairClasses = 10;
+constexpr int kQuartetClasses = 55;
+__host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+__host__ __device__ constexpr int pc_la(int pc) { return pc >= 6 ? 3 : pc >= 3 ? 2 : pc >= 1 ? 1 : 0; }
+__host__ __device__ constexpr int pc_lb(int pc) { return pc - pc_la(pc) * (pc_la(pc) + 1) / 2; }
+__host__ __device__ constexpr int quartet_class(int bra_pc, int ket_pc) { return bra_pc * (bra_pc + 1) / 2 + ket_pc; }
+
+// One launcher per quartet class.  nk = number of exchange densities (1 or 2).
+using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, cudaStream_t st);
+
+// pfk_classes.cu, compiled once per bra class; a launcher called with
+// n < 0 only configures the current device for its kernels.
+void register_bra_class_0(ClassLauncher *table);
+void register_bra_class_1(ClassLauncher *table);
+void register_bra_class_2(ClassLauncher *table);
+void register_bra_class_3(ClassLauncher *table);
+void register_bra_class_4(ClassLauncher *table);
+void register_bra_class_5(ClassLauncher *table);
+void register_bra_class_6(ClassLauncher *table);
+void register_bra_class_7(ClassLauncher *table);
+void register_bra_class_8(ClassLauncher *table);
+void register_bra_class_9(ClassLauncher *table);
+
+}  // namespace pfk

@@ -1,0 +1,429 @@
+// pfk_kernels.cuh -- per-angular-momentum-class ERI + J/K kernels.
+//
+// A class is (LA LB | LC LD) with LA >= LB, LC >= LD and (LA,LB) >= (LC,LD)
+// in pair-class order; 55 classes cover (ss|ss)..(ff|ff).  Each kernel walks
+// a list of screened shell quartets (bra pair, ket pair) of its class.
+//
+//   eri_reg_kernel   one thread per shell quartet; the contracted Cartesian
+//                    block, the per-root axis tables and the J/K partial
+//                    sums all live in registers.  Used for small classes.
+//   eri_team_kernel  a team of TEAM threads (a warp or the whole block) per
+//                    shell quartet; the per-root axis tables are built once
+//                    per primitive quartet into shared memory and every
+//                    thread accumulates a strided slice of the components.
+#pragma once
+#include "pfk_device.cuh"
+
+namespace pfk {
+
+template <int LA, int LB, int LC, int LD>
+struct ClassShape {
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    static constexpr int N = NA * NB * NC * ND;
+    static constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    static constexpr int NI = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+    // offsets of component (ia, ib, ic, id) in the per-axis tables
+    __host__ __device__ static constexpr int ax(int ia, int ib, int ic, int id)
+    {
+        return ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib)) * (LC + 1) + cart_lx(LC, ic)) * (LD + 1) + cart_lx(LD, id);
+    }
+    __host__ __device__ static constexpr int ay(int ia, int ib, int ic, int id)
+    {
+        return ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib)) * (LC + 1) + cart_ly(LC, ic)) * (LD + 1) + cart_ly(LD, id);
+    }
+    __host__ __device__ static constexpr int az(int ia, int ib, int ic, int id)
+    {
+        return ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib)) * (LC + 1) + cart_lz(LC, ic)) * (LD + 1) + cart_lz(LD, id);
+    }
+    __host__ __device__ static constexpr double norm(int ia, int ib, int ic, int id)
+    {
+        return cart_norm(LA, ia) * cart_norm(LB, ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+    }
+};
+
+// Canonical-quartet bookkeeping for one Cartesian component quartet.
+// Returns the weight s (0 when the component is a duplicate or screened out).
+__device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, bool same_bk, int ia, int ib,
+                                                 int ic, int id, int NBc, int NDc, bool check,
+                                                 const double *__restrict__ Qao, int nb, int i, int j,
+                                                 int k, int l, double tol)
+{
+    double s = 1.0;
+    if (same_ab) {
+        if (ia > ib) return 0.0;
+        if (ia == ib) s *= 0.5;
+    }
+    if (same_cd) {
+        if (ic > id) return 0.0;
+        if (ic == id) s *= 0.5;
+    }
+    if (same_bk) {
+        const int pb = ia * NBc + ib, pk = ic * NDc + id;
+        if (pb > pk) return 0.0;
+        if (pb == pk) s *= 0.5;
+    }
+    if (check && __ldg(Qao + (size_t)i * nb + j) * __ldg(Qao + (size_t)k * nb + l) < tol) return 0.0;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Register path
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, int NK>
+__global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
+{
+    using S = ClassShape<LA, LB, LC, LD>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    const uint2 qd = quartets[t];
+    const PairInfo pb = args.pairs[qd.x];
+    const PairInfo pk = args.pairs[qd.y];
+
+    double acc[NA * NB * NC * ND];
+#pragma unroll
+    for (int c = 0; c < S::N; ++c) acc[c] = 0.0;
+
+    for (int ip = 0; ip < pb.nprim; ++ip) {
+        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+        for (int jp = 0; jp < pk.nprim; ++jp) {
+            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+            const QuartetScalars s = quartet_scalars(p, q);
+            double u[NR], w[NR];
+            rys_roots<NR>(s.T, u, w);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const double ur = u[r];
+                const double B00 = 0.5 * s.rdelta * ur;
+                const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
+                const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
+                double gx[NI], gy[NI], gz[NI];
+                axis_table<LA, LB, LC, LD, double>(p.PAx + ur * s.WPx, q.PAx + ur * s.WQx, B00, B10, B01,
+                                                   pb.ABx, pk.ABx, w[r] * s.pref, gx);
+                axis_table<LA, LB, LC, LD, double>(p.PAy + ur * s.WPy, q.PAy + ur * s.WQy, B00, B10, B01,
+                                                   pb.ABy, pk.ABy, 1.0, gy);
+                axis_table<LA, LB, LC, LD, double>(p.PAz + ur * s.WPz, q.PAz + ur * s.WQz, B00, B10, B01,
+                                                   pb.ABz, pk.ABz, 1.0, gz);
+#pragma unroll
+                for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                    for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                            for (int id = 0; id < ND; ++id) {
+                                const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                                acc[c] += gx[S::ax(ia, ib, ic, id)] * gy[S::ay(ia, ib, ic, id)] *
+                                          gz[S::az(ia, ib, ic, id)];
+                            }
+            }
+        }
+    }
+
+    // ---- digestion ----
+    const int nb = args.nb;
+    const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
+    const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
+    const bool check = pb.qmin * pk.qmin < args.tol;
+
+    if (args.eri_out) {
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) {
+                        const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                        const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
+                                                         args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
+                        if (sw != 0.0)
+                            scatter8(args.eri_out, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id,
+                                     acc[c] * S::norm(ia, ib, ic, id));
+                    }
+        return;
+    }
+
+    const double *__restrict__ Pj = args.Pj;
+    double jab[NA * NB], jcd[NC * ND];
+    double pab[NA * NB], pcd[NC * ND];
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+            jab[ia * NB + ib] = 0.0;
+            pab[ia * NB + ib] = __ldg(Pj + (size_t)(i0 + ia) * nb + j0 + ib);
+        }
+#pragma unroll
+    for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+        for (int id = 0; id < ND; ++id) {
+            jcd[ic * ND + id] = 0.0;
+            pcd[ic * ND + id] = __ldg(Pj + (size_t)(k0 + ic) * nb + l0 + id);
+        }
+    // exchange: four blocks per K density
+    double kac[NK][NA * NC], kbc[NK][NB * NC], kad[NK][NA * ND], kbd[NK][NB * ND];
+    double pac[NK][NA * NC], pbc[NK][NB * NC], pad_[NK][NA * ND], pbd[NK][NB * ND];
+#pragma unroll
+    for (int m = 0; m < NK; ++m) {
+        const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) {
+                kac[m][ia * NC + ic] = 0.0;
+                pac[m][ia * NC + ic] = __ldg(Pk + (size_t)(i0 + ia) * nb + k0 + ic);
+            }
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) {
+                kbc[m][ib * NC + ic] = 0.0;
+                pbc[m][ib * NC + ic] = __ldg(Pk + (size_t)(j0 + ib) * nb + k0 + ic);
+            }
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) {
+                kad[m][ia * ND + id] = 0.0;
+                pad_[m][ia * ND + id] = __ldg(Pk + (size_t)(i0 + ia) * nb + l0 + id);
+            }
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) {
+                kbd[m][ib * ND + id] = 0.0;
+                pbd[m][ib * ND + id] = __ldg(Pk + (size_t)(j0 + ib) * nb + l0 + id);
+            }
+    }
+
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                    const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
+                                                     args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
+                    const double v = acc[c] * (sw * S::norm(ia, ib, ic, id));
+                    jab[ia * NB + ib] += v * pcd[ic * ND + id];
+                    jcd[ic * ND + id] += v * pab[ia * NB + ib];
+#pragma unroll
+                    for (int m = 0; m < NK; ++m) {
+                        kac[m][ia * NC + ic] += v * pbd[m][ib * ND + id];
+                        kbc[m][ib * NC + ic] += v * pad_[m][ia * ND + id];
+                        kad[m][ia * ND + id] += v * pbc[m][ib * NC + ic];
+                        kbd[m][ib * ND + id] += v * pac[m][ia * NC + ic];
+                    }
+                }
+
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, jab[ia * NB + ib]);
+#pragma unroll
+    for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+        for (int id = 0; id < ND; ++id) atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, jcd[ic * ND + id]);
+#pragma unroll
+    for (int m = 0; m < NK; ++m) {
+        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+        if (!Kacc) continue;
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(i0 + ia) * nb + k0 + ic, kac[m][ia * NC + ic]);
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(j0 + ib) * nb + k0 + ic, kbc[m][ib * NC + ic]);
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(i0 + ia) * nb + l0 + id, kad[m][ia * ND + id]);
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(j0 + ib) * nb + l0 + id, kbd[m][ib * ND + id]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Team path (TEAM = 32: one warp per quartet, 4 per block; TEAM = 128: the
+// whole block per quartet).
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD>
+struct TeamShape {
+    using S = ClassShape<LA, LB, LC, LD>;
+    static constexpr int TEAM = S::N <= 1300 ? 32 : 128;
+    static constexpr int TEAMS = 128 / TEAM;
+    static constexpr int KPT = (S::N + TEAM - 1) / TEAM;
+    static constexpr int TABLE = S::NR * 3 * S::NI;          // doubles per team
+    static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
+};
+
+template <int TEAM>
+__device__ __forceinline__ void team_sync()
+{
+    if constexpr (TEAM == 32) __syncwarp();
+    else __syncthreads();
+}
+
+template <int LA, int LB, int LC, int LD, int NK>
+__global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
+{
+    using S = ClassShape<LA, LB, LC, LD>;
+    using TS = TeamShape<LA, LB, LC, LD>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
+    constexpr int TEAM = TS::TEAM, KPT = TS::KPT;
+    extern __shared__ double smem[];
+    const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
+    const long long t = (long long)blockIdx.x * TS::TEAMS + team;
+    // TEAM == 32 teams are whole warps and may leave together; the block-wide
+    // team has exactly one quartet per block, so no thread waits on a leaver.
+    if (t >= nq) return;
+    double *g = smem + team * TS::TABLE;   // g[r][axis][NI]
+
+    const uint2 qd = quartets[t];
+    const PairInfo pb = args.pairs[qd.x];
+    const PairInfo pk = args.pairs[qd.y];
+
+    int off[KPT];
+    double acc[KPT];
+#pragma unroll
+    for (int k = 0; k < KPT; ++k) {
+        acc[k] = 0.0;
+        const int c = lane + k * TEAM;
+        if (c < S::N) {
+            const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
+            const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib)) * (LC + 1) + cart_lx(LC, ic)) * (LD + 1) + cart_lx(LD, id);
+            const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib)) * (LC + 1) + cart_ly(LC, ic)) * (LD + 1) + cart_ly(LD, id);
+            const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib)) * (LC + 1) + cart_lz(LC, ic)) * (LD + 1) + cart_lz(LD, id);
+            off[k] = ox | (oy << 10) | (oz << 20);
+        } else {
+            off[k] = 0;
+        }
+    }
+
+    for (int ip = 0; ip < pb.nprim; ++ip) {
+        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+        for (int jp = 0; jp < pk.nprim; ++jp) {
+            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+            const QuartetScalars s = quartet_scalars(p, q);
+            for (int task = lane; task < 3 * NR; task += TEAM) {
+                const int r = task / 3, axis = task - 3 * r;
+                double ur, wr;
+                rys_root_one<NR>(s.T, r, ur, wr);
+                const double B00 = 0.5 * s.rdelta * ur;
+                const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
+                const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
+                double C00, D00, AB, CD, scale = 1.0;
+                if (axis == 0) { C00 = p.PAx + ur * s.WPx; D00 = q.PAx + ur * s.WQx; AB = pb.ABx; CD = pk.ABx; scale = wr * s.pref; }
+                else if (axis == 1) { C00 = p.PAy + ur * s.WPy; D00 = q.PAy + ur * s.WQy; AB = pb.ABy; CD = pk.ABy; }
+                else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
+                axis_table<LA, LB, LC, LD, double>(C00, D00, B00, B10, B01, AB, CD, scale, g + (r * 3 + axis) * NI);
+            }
+            team_sync<TEAM>();
+#pragma unroll
+            for (int k = 0; k < KPT; ++k) {
+                const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
+                double a = acc[k];
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    a += g[(r * 3 + 0) * NI + ox] * g[(r * 3 + 1) * NI + oy] * g[(r * 3 + 2) * NI + oz];
+                acc[k] = a;
+            }
+            team_sync<TEAM>();
+        }
+    }
+
+    const int nb = args.nb;
+    const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
+    const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
+    const bool check = pb.qmin * pk.qmin < args.tol;
+#pragma unroll
+    for (int k = 0; k < KPT; ++k) {
+        const int c = lane + k * TEAM;
+        if (c >= S::N) continue;
+        const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
+        const int i = i0 + ia, j = j0 + ib, kk = k0 + ic, l = l0 + id;
+        const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao, nb,
+                                         i, j, kk, l, args.tol);
+        if (sw == 0.0) continue;
+        const double v = acc[k] * sw * cart_norm(LA, ia) * cart_norm(LB, ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+        if (args.eri_out) {
+            scatter8(args.eri_out, nb, i, j, kk, l, v / sw);
+            continue;
+        }
+        atomicAdd(args.Jacc + (size_t)i * nb + j, v * __ldg(args.Pj + (size_t)kk * nb + l));
+        atomicAdd(args.Jacc + (size_t)kk * nb + l, v * __ldg(args.Pj + (size_t)i * nb + j));
+#pragma unroll
+        for (int m = 0; m < NK; ++m) {
+            double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+            const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
+            if (!Kacc) continue;
+            atomicAdd(Kacc + (size_t)i * nb + kk, v * __ldg(Pk + (size_t)j * nb + l));
+            atomicAdd(Kacc + (size_t)j * nb + kk, v * __ldg(Pk + (size_t)i * nb + l));
+            atomicAdd(Kacc + (size_t)i * nb + l, v * __ldg(Pk + (size_t)j * nb + kk));
+            atomicAdd(Kacc + (size_t)j * nb + l, v * __ldg(Pk + (size_t)i * nb + kk));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Schwarz diagonal (ab|ab) per shell pair of class (LA, LB): Q(i,j) for all
+// component pairs (os.cpp:1703-1752, rys.cpp:509-556).
+// ---------------------------------------------------------------------------
+template <int LA, int LB>
+__global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pair_ids, int n, const PairInfo *__restrict__ pairs,
+                                                     const PrimPair *__restrict__ prims, double *Qao, int nb)
+{
+    using S = ClassShape<LA, LB, LA, LB>;
+    constexpr int NA = S::NA, NB = S::NB, NR = S::NR, NI = S::NI;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const PairInfo pb = pairs[pair_ids[t]];
+    double acc[NA * NB];
+#pragma unroll
+    for (int c = 0; c < NA * NB; ++c) acc[c] = 0.0;
+    for (int ip = 0; ip < pb.nprim; ++ip) {
+        const PrimPair p = load_prim(prims, pb.prim_off + ip);
+        for (int jp = 0; jp < pb.nprim; ++jp) {
+            const PrimPair q = load_prim(prims, pb.prim_off + jp);
+            const QuartetScalars s = quartet_scalars(p, q);
+            double u[NR], w[NR];
+            rys_roots<NR>(s.T, u, w);
+            for (int r = 0; r < NR; ++r) {
+                const double ur = u[r];
+                const double B00 = 0.5 * s.rdelta * ur;
+                const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
+                const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
+                double gx[NI], gy[NI], gz[NI];
+                axis_table<LA, LB, LA, LB, double>(p.PAx + ur * s.WPx, q.PAx + ur * s.WQx, B00, B10, B01, pb.ABx, pb.ABx, w[r] * s.pref, gx);
+                axis_table<LA, LB, LA, LB, double>(p.PAy + ur * s.WPy, q.PAy + ur * s.WQy, B00, B10, B01, pb.ABy, pb.ABy, 1.0, gy);
+                axis_table<LA, LB, LA, LB, double>(p.PAz + ur * s.WPz, q.PAz + ur * s.WQz, B00, B10, B01, pb.ABz, pb.ABz, 1.0, gz);
+#pragma unroll
+                for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                    for (int ib = 0; ib < NB; ++ib)
+                        acc[ia * NB + ib] += gx[S::ax(ia, ib, ia, ib)] * gy[S::ay(ia, ib, ia, ib)] * gz[S::az(ia, ib, ia, ib)];
+            }
+        }
+    }
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+            const double nrm = cart_norm(LA, ia) * cart_norm(LB, ib);
+            const double q = sqrt(fabs(acc[ia * NB + ib] * nrm * nrm));
+            const int i = pb.bf_a + ia, j = pb.bf_b + ib;
+            Qao[(size_t)i * nb + j] = q;
+            Qao[(size_t)j * nb + i] = q;
+        }
+}
+
+}  // namespace pfk

@@ -1,0 +1,23 @@
+// pfk_setup.h -- host wrappers of the setup and finishing kernels (pfk_setup.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pfk_device.cuh"
+
+namespace pfk {
+
+void launch_schwarz(int pc, const int *ids, int n, const PairInfo *pairs, const PrimPair *prims, double *Q, int nb,
+                    cudaStream_t st);
+cudaError_t count_quartets(const double *qX, int nX, const double *qY, int nY, int diag, double tol, double bound,
+                           long long *cnt_hi, long long *cnt_lo, cudaStream_t st);
+cudaError_t exclusive_scan(const long long *in, long long *out, int n, void *tmp, size_t &tmp_bytes, cudaStream_t st);
+cudaError_t fill_quartets(const int *idX, int nX, const int *idY, int diag, const long long *off_hi,
+                          const long long *cnt_hi, const long long *off_lo, const long long *cnt_lo, uint2 *out_hi,
+                          uint2 *out_lo, cudaStream_t st);
+cudaError_t census(const uint2 *q, long long nq, const PairInfo *pairs, const int *pair_la, const int *pair_lb,
+                   const double *Qao, int nb, double tol, unsigned long long *counters, int *out, long long cap,
+                   cudaStream_t st);
+cudaError_t combine(const double *J, const double *K, double cj, double ck, double *out, int nb, cudaStream_t st);
+cudaError_t add(const double *a, const double *b, double *out, long long n, cudaStream_t st);
+
+}  // namespace pfk

@@ -20,7 +20,10 @@ ill-conditioned in double precision, so this script runs it once, offline, in
     to better than 1e-15 relative (checked below).
 
 Output: csrc/rys_table_data.inc (C initialisers, committed; regenerate with
-`python gen_rys_table.py`).  The script also prints the measured maximum
+`python gen_rys_table.py`).  The includer defines PFK_RYS_CONST_STORAGE and
+PFK_RYS_TABLE_STORAGE (e.g. `static __constant__ const` and
+`static __device__ const`) so every translation unit gets statically
+initialised device copies.  The script also prints the measured maximum
 interpolation error at random T against fresh 80-digit evaluations.
 """
 import multiprocessing as mproc
@@ -183,16 +186,16 @@ def main():
             f.write(f"//   n={n}: {worst[n]:.3e}\n")
         f.write(f"#define PFK_RYS_NMAX {NMAX}\n#define PFK_RYS_DEG {DEG}\n")
         f.write(f"#define PFK_RYS_H {H!r}\n")
-        f.write("static const double kRysTmax[PFK_RYS_NMAX + 1] = {0.0, " +
+        f.write("PFK_RYS_CONST_STORAGE double kRysTmax[PFK_RYS_NMAX + 1] = {0.0, " +
                 ", ".join(repr(TMAX[n]) for n in range(1, NMAX + 1)) + "};\n")
         off = 0
         offs = [0]
         for n in range(1, NMAX + 1):
             offs.append(off)
             off += layout[n - 1] * 2 * n * N
-        f.write("static const int kRysOffset[PFK_RYS_NMAX + 1] = {" + ", ".join(str(o) for o in offs) + "};\n")
+        f.write("PFK_RYS_CONST_STORAGE int kRysOffset[PFK_RYS_NMAX + 1] = {" + ", ".join(str(o) for o in offs) + "};\n")
         f.write(f"#define PFK_RYS_TABLE_SIZE {off}\n")
-        f.write("static const double kRysCheb[PFK_RYS_TABLE_SIZE] = {\n")
+        f.write("PFK_RYS_TABLE_STORAGE double kRysCheb[PFK_RYS_TABLE_SIZE] = {\n")
         for n in range(1, NMAX + 1):
             f.write(f"// n = {n}: {layout[n-1]} intervals x {2*n} values x {N} coefficients\n")
             for i in range(layout[n - 1]):
@@ -200,14 +203,14 @@ def main():
                     f.write(",".join(f"{c:.17g}" for c in tables[n][i][v]) + ",\n")
         f.write("};\n")
         # large-T limit constants: x_i^2 and W_i for each n
-        f.write("static const double kRysAsymU[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")
+        f.write("PFK_RYS_CONST_STORAGE double kRysAsymU[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")
         asym_w = []
         for n in range(1, NMAX + 1):
             x2, W = half_hermite(n)
             f.write("  {" + ", ".join(f"{float(x):.17g}" for x in x2) + "},\n")
             asym_w.append(W)
         f.write("};\n")
-        f.write("static const double kRysAsymW[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")
+        f.write("PFK_RYS_CONST_STORAGE double kRysAsymW[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")
         for W in asym_w:
             f.write("  {" + ", ".join(f"{float(x):.17g}" for x in W) + "},\n")
         f.write("};\n")
