@@ -125,9 +125,27 @@ pfk_status pfk_fock_rhf_device(pfk_ctx *ctx, const double *dP, double *dG, void 
  * (_compute_2e, os.cpp:1755-1829).  Host buffer of nb^4 doubles. */
 pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri);
 
-/* Per-class shell-quartet counts (55 classes (ss|ss)..(ff|ff)) and the
- * device time of the last build per class in milliseconds, for profiling. */
-pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, double *ms55);
+/* Per-class work of one build over the 55 classes (ss|ss)..(ff|ff):
+ * screened shell quartets, primitive quartets (sum of K_ab * K_cd), and --
+ * when ms55 is non-null -- the device time of each class's kernel in a
+ * timed RHF build on the context's current density, in milliseconds.
+ * Any output pointer may be NULL.  For profiling and roofline reports. */
+pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_quartets55,
+                           double *ms55);
+
+/* Restrict every later build of this context to shard `rank` of `nranks`:
+ * each class's screened quartet list is cut into nranks contiguous slices
+ * of equal primitive-quartet work and only slice `rank` is evaluated, so the
+ * partial G (or J, K) of all ranks sum to the full result.  nranks = 1
+ * restores the whole list.  Used by one-process-per-GPU runs, which sum the
+ * partial matrices with one all-reduce. */
+pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
+
+/* Measurement helper: sustained FP64 and FP32 fused-multiply-add throughput
+ * of `device` in TFLOP/s (2 flops per FMA), from a register-resident FMA
+ * loop over all SMs, timed with CUDA events.  The FP64 figure is the
+ * roofline denominator of the integral kernels. */
+pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 #ifdef __cplusplus
 }

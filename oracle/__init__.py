@@ -69,6 +69,10 @@ def lib():
             L.orc_fock_uhf_from_tensor.argtypes = [ctypes.c_size_t, vp, vp, vp, vp, vp]
             L.orc_jk_direct.restype = ctypes.c_longlong
             L.orc_jk_direct.argtypes = [vp, c_dbl, c_int, vp, c_int, vp, vp, vp, vp, c_int, c_int]
+            L.orc_jk_direct_rows.restype = ctypes.c_longlong
+            L.orc_jk_direct_rows.argtypes = [vp, c_dbl, c_int, vp, c_int, vp, vp, vp, vp, vp, c_int]
+            L.orc_row_count.restype = ctypes.c_longlong
+            L.orc_row_count.argtypes = [vp, c_dbl, vp, c_int]
             L.orc_quartet_list.restype = ctypes.c_longlong
             L.orc_quartet_list.argtypes = [vp, c_dbl, vp, vp, vp, ctypes.c_longlong]
             L.orc_one_electron.argtypes = [vp, c_int, vp, vp, vp, vp]
@@ -94,7 +98,7 @@ def rys_roots(n, T):
 
 
 def load_basis_library():
-    with open(os.path.join(GOLDEN, "basis_sets.json")) as f:
+    with open(os.path.join(REPO, "planck-refactored_b200", "data", "basis_sets.json")) as f:
         return json.load(f)["basis"]
 
 
@@ -215,6 +219,23 @@ class Basis:
         n = lib().orc_jk_direct(self.h, tol, engine, _p(Q), len(Pk_list), _p(Pj), _p(Pk),
                                 _p(J), _p(K), pair_range[0], pair_range[1])
         return J, K, n
+
+    def jk_direct_rows(self, Pj, Pk_list, rows, tol=1e-10, engine=OS, Q=None):
+        """Streaming J/K restricted to the given bra AO-pair rows."""
+        if Q is None:
+            Q = self.schwarz(engine)
+        nb = self.nbasis
+        Pj = np.ascontiguousarray(Pj, dtype=np.float64)
+        Pk = np.ascontiguousarray(np.stack(Pk_list), dtype=np.float64)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        J = np.zeros((nb, nb))
+        K = np.zeros((len(Pk_list), nb, nb))
+        n = lib().orc_jk_direct_rows(self.h, tol, engine, _p(Q), len(Pk_list), _p(Pj), _p(Pk),
+                                     _p(J), _p(K), _p(rows), len(rows))
+        return J, K, n
+
+    def row_count(self, p, tol, Q):
+        return lib().orc_row_count(self.h, tol, _p(Q), int(p))
 
     def eri_pair(self, p, q, engine=OS):
         return lib().orc_eri_pair(self.h, p, q, engine)

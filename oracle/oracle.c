@@ -1021,14 +1021,11 @@ void orc_fock_uhf_from_tensor(size_t nb, const double *eri, const double *Pa, co
 /* J and K are accumulated separately: G_rhf = J - K/2; for UHF with         */
 /* Pa, Pb: Ga = J(Pa+Pb) - K(Pa), Gb = J(Pa+Pb) - K(Pb).                    */
 /* ------------------------------------------------------------------------ */
-long long orc_jk_direct(const orc_basis *b, double tol, int engine, const double *Q,
-                        int nmat, const double *Pj, const double *Pk, double *J, double *K,
-                        int pair_begin, int pair_end)
+static long long jk_rows(const orc_basis *b, double tol, int engine, const double *Q, int nmat, const double *Pj,
+                         const double *Pk, double *J, double *K, const int *rows, int nrows, int row_begin)
 {
     const int nb = b->nbasis;
     const size_t nb2 = (size_t)nb * nb;
-    if (pair_end < 0 || pair_end > b->npairs)
-        pair_end = b->npairs;
     long long count = 0;
     memset(J, 0, sizeof(double) * nb2);
     memset(K, 0, sizeof(double) * nb2 * nmat);
@@ -1037,7 +1034,8 @@ long long orc_jk_direct(const orc_basis *b, double tol, int engine, const double
         double *Jl = calloc(nb2, sizeof(double));
         double *Kl = calloc(nb2 * nmat, sizeof(double));
 #pragma omp for schedule(dynamic)
-        for (int p = pair_begin; p < pair_end; ++p) {
+        for (int r = 0; r < nrows; ++r) {
+            const int p = rows ? rows[r] : row_begin + r;
             const orc_pair *ab = &b->pairs[p];
             for (int q = p; q < b->npairs; ++q) {
                 const orc_pair *cd = &b->pairs[q];
@@ -1055,11 +1053,11 @@ long long orc_jk_direct(const orc_basis *b, double tol, int engine, const double
                               perm[c][2] == perm[a][2] && perm[c][3] == perm[a][3];
                     if (dup)
                         continue;
-                    const int m = perm[a][0], n = perm[a][1], r = perm[a][2], s = perm[a][3];
+                    const int m = perm[a][0], n = perm[a][1], rr = perm[a][2], s = perm[a][3];
                     /* (mn|rs): J(m,n) += P(r,s) v ; K(m,r) += P(n,s) v */
-                    Jl[(size_t)m * nb + n] += Pj[(size_t)r * nb + s] * v;
+                    Jl[(size_t)m * nb + n] += Pj[(size_t)rr * nb + s] * v;
                     for (int t = 0; t < nmat; ++t)
-                        Kl[t * nb2 + (size_t)m * nb + r] += Pk[t * nb2 + (size_t)n * nb + s] * v;
+                        Kl[t * nb2 + (size_t)m * nb + rr] += Pk[t * nb2 + (size_t)n * nb + s] * v;
                 }
             }
         }
@@ -1074,6 +1072,40 @@ long long orc_jk_direct(const orc_basis *b, double tol, int engine, const double
         free(Kl);
     }
     return count;
+}
+
+long long orc_jk_direct(const orc_basis *b, double tol, int engine, const double *Q,
+                        int nmat, const double *Pj, const double *Pk, double *J, double *K,
+                        int pair_begin, int pair_end)
+{
+    if (pair_end < 0 || pair_end > b->npairs)
+        pair_end = b->npairs;
+    if (pair_begin < 0)
+        pair_begin = 0;
+    return jk_rows(b, tol, engine, Q, nmat, Pj, Pk, J, K, NULL,
+                   pair_end > pair_begin ? pair_end - pair_begin : 0, pair_begin);
+}
+
+/* The same over an explicit list of bra AO-pair rows (a bounded sample). */
+long long orc_jk_direct_rows(const orc_basis *b, double tol, int engine, const double *Q,
+                             int nmat, const double *Pj, const double *Pk, double *J, double *K,
+                             const int *rows, int nrows)
+{
+    return jk_rows(b, tol, engine, Q, nmat, Pj, Pk, J, K, rows, nrows, 0);
+}
+
+/* Number of screened canonical AO quartets in bra row p (q >= p). */
+long long orc_row_count(const orc_basis *b, double tol, const double *Q, int p)
+{
+    const int nb = b->nbasis;
+    const orc_pair *ab = &b->pairs[p];
+    const double qa = Q[ab->i * nb + ab->j];
+    long long c = 0;
+    for (int q = p; q < b->npairs; ++q) {
+        const orc_pair *cd = &b->pairs[q];
+        c += !(qa * Q[cd->i * nb + cd->j] < tol);
+    }
+    return c;
 }
 
 /* ------------------------------------------------------------------------ */

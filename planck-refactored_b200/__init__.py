@@ -16,6 +16,7 @@ import os
 
 import numpy as np
 
+from . import workloads  # noqa: F401
 from .basis import (ANGSTROM_TO_BOHR, Molecule, cartesian_order, component_norm,  # noqa: F401
                     read_gbs_basis, shells_for)
 
@@ -28,7 +29,7 @@ ENGINES = {"os": 0, "rys": 1, "auto": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
-           "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats"]
+           "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak"]
 
 _lib = None
 
@@ -70,7 +71,9 @@ def load_library(path=LIB_PATH):
     L.pfk_jk.argtypes = [vp, vp, vp, vp, vp, c_dbl]
     L.pfk_fock_rhf_device.argtypes = [vp, vp, vp, vp]
     L.pfk_eri_tensor.argtypes = [vp, vp]
-    L.pfk_class_stats.argtypes = [vp, vp, vp]
+    L.pfk_class_stats.argtypes = [vp, vp, vp, vp]
+    L.pfk_set_shard.argtypes = [vp, c_int, c_int]
+    L.pfk_measure_fma_peak.argtypes = [c_int, ctypes.POINTER(c_dbl), ctypes.POINTER(c_dbl)]
     _lib = L
     return L
 
@@ -184,10 +187,39 @@ class FockEngine:
         return eri
 
     def class_stats(self, timed=True):
+        """{class name: (shell quartets, primitive quartets, ms)} for non-empty classes."""
         q = np.zeros(55, dtype=np.int64)
+        k = np.zeros(55, dtype=np.int64)
         ms = np.zeros(55)
-        self._check(self.lib.pfk_class_stats(self.h, _p(q), _p(ms) if timed else None))
-        return {CLASS_NAMES[c]: (int(q[c]), float(ms[c])) for c in range(55) if q[c]}
+        self._check(self.lib.pfk_class_stats(self.h, _p(q), _p(k), _p(ms) if timed else None))
+        return {CLASS_NAMES[c]: (int(q[c]), int(k[c]), float(ms[c])) for c in range(55) if q[c]}
+
+    def set_shard(self, rank, nranks):
+        self._check(self.lib.pfk_set_shard(self.h, int(rank), int(nranks)))
+
+
+def measure_fma_peak(device=0):
+    """(FP64, FP32) FMA throughput of the device in TFLOP/s."""
+    L = load_library()
+    a, b = ctypes.c_double(), ctypes.c_double()
+    st = L.pfk_measure_fma_peak(int(device), ctypes.byref(a), ctypes.byref(b))
+    if st != PFK_OK:
+        raise PfkError(st, L.pfk_last_error(None).decode())
+    return a.value, b.value
+
+
+def class_flops(name, prim_quartets):
+    """Algorithmic FP64 work of a class: K * n_r * [12 (e+1)(f+1) +
+    6 (la+1)(lb+1)(lc+1)(ld+1) + 3 N] + 40 K (K = primitive quartets,
+    e = la+lb, f = lc+ld, n_r = (e+f)//2 + 1, N = Cartesian block size)."""
+    l = {"s": 0, "p": 1, "d": 2, "f": 3}
+    la, lb, lc, ld = l[name[1]], l[name[2]], l[name[4]], l[name[5]]
+    e, f = la + lb, lc + ld
+    nr = (e + f) // 2 + 1
+    nc = lambda x: (x + 1) * (x + 2) // 2
+    N = nc(la) * nc(lb) * nc(lc) * nc(ld)
+    return prim_quartets * nr * (12 * (e + 1) * (f + 1) + 6 * (la + 1) * (lb + 1) * (lc + 1) * (ld + 1) + 3 * N) \
+        + 40 * prim_quartets
 
 
 # ---------------------------------------------------------------------------

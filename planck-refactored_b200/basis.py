@@ -11,11 +11,25 @@ the C ABI consumes:
   * Cartesian order lx descending then ly descending (basis.cpp:20-37) and
     component norms 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!) (gaussian.cpp:283-296).
 """
+import json
+import os
+
 import numpy as np
 
 ANGSTROM_TO_BOHR = 1.8897259886
 ZNUC = {"H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Ne": 10}
 _PI = 3.1415926535897932384626433832795
+
+
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "basis_sets.json")
+
+
+def load_library(path=DATA):
+    """Parsed basis sets {name: {element: [[L, [[exponent, raw coefficient], ...]], ...]}}
+    for H, C, N, O in sto-3g, 3-21g, 6-31g*, 6-31g**, cc-pvdz (Basis Set
+    Exchange data, SP shells split into S and P as the reference's parser does)."""
+    with open(path) as f:
+        return json.load(f)["basis"]
 
 
 class Molecule:

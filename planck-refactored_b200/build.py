@@ -9,7 +9,6 @@ or include/ is newer than them.
 """
 import argparse
 import concurrent.futures as cf
-import glob
 import os
 import subprocess
 import sys
@@ -25,14 +24,22 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC,
          "-I" + os.path.join(REPO, "include")]
 
 
+DEVICE_DEPS = ["pfk_device.cuh", "pfk_internal.h", "rys_table_data.inc"]
+DEPS = {
+    "pfk_classes.cu": DEVICE_DEPS + ["pfk_kernels.cuh"],
+    "pfk_setup.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_setup.h"],
+    "pfk_api.cu": DEVICE_DEPS + ["pfk_setup.h", "../../include/planck_fock.h"],
+}
+
+
 def _units():
     units = [("pfk_classes.cu", f"classes_{x}.o", [f"-DPFK_BRA_CLASS={x}"]) for x in range(9, -1, -1)]
     units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", [])]
     return units
 
 
-def _newest_source():
-    files = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(REPO, "include", "*.h"))
+def _newest(src):
+    files = [os.path.join(CSRC, src)] + [os.path.join(CSRC, d) for d in DEPS[src]] + [os.path.abspath(__file__)]
     return max(os.path.getmtime(f) for f in files)
 
 
@@ -48,11 +55,10 @@ def _compile(src, obj, extra, verbose):
 
 def build(jobs=None, force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
-    newest = _newest_source()
     todo = []
     for src, obj, extra in _units():
         path = os.path.join(BUILD, obj)
-        if force or not os.path.exists(path) or os.path.getmtime(path) < newest:
+        if force or not os.path.exists(path) or os.path.getmtime(path) < _newest(src):
             todo.append((src, path, extra))
     logs = {}
     if todo:

@@ -69,6 +69,15 @@ struct pfk_ctx {
     std::vector<int> cls_ids[kPairClasses];
     DevBuf<int> d_cls_ids[kPairClasses];
     DevBuf<double> d_cls_q[kPairClasses];
+    DevBuf<long long> d_cls_kpref[kPairClasses];   // prefix of nprim over the sorted class list
+
+    // per quartet class, per bra: prefix of quartet counts and of primitive
+    // work for the FP64 ("hi") and FP32 ("lo") lists (size nX + 1)
+    std::vector<long long> qpref_hi[kQuartetClasses], qpref_lo[kQuartetClasses];
+    std::vector<long long> wpref_hi[kQuartetClasses], wpref_lo[kQuartetClasses];
+    long long prim_cnt[kQuartetClasses] = {};
+    int shard_rank = 0, shard_n = 1;
+    long long sl_hi[kQuartetClasses][2] = {}, sl_lo[kQuartetClasses][2] = {};   // [begin, count) of this shard
 
     double tol = 1e-10, fp32_bound = 1e-8;
     int engine = PFK_ENGINE_OS, precision = PFK_PREC_FP64;
@@ -199,13 +208,48 @@ pfk_status upload_pairs(pfk_ctx *ctx)
     return PFK_OK;
 }
 
+// This shard's slice of each class list: bra boundaries splitting the
+// primitive work into shard_n equal parts.
+void slice_one(const std::vector<long long> &qp, const std::vector<long long> &wp, int r, int n, long long out[2])
+{
+    out[0] = out[1] = 0;
+    if (qp.empty()) return;
+    const long long W = wp.back();
+    auto bound = [&](int k) -> size_t {
+        if (k <= 0) return 0;
+        if (k >= n) return wp.size() - 1;
+        const long long t = (long long)((double)W * k / n);
+        return (size_t)(std::lower_bound(wp.begin(), wp.end(), t) - wp.begin());
+    };
+    const size_t a0 = bound(r), a1 = std::max(a0, bound(r + 1));
+    out[0] = qp[a0];
+    out[1] = qp[a1] - qp[a0];
+}
+
+void compute_slices(pfk_ctx *ctx)
+{
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        if (ctx->shard_n <= 1) {
+            ctx->sl_hi[c][0] = 0;
+            ctx->sl_hi[c][1] = ctx->q_cnt[c];
+            ctx->sl_lo[c][0] = 0;
+            ctx->sl_lo[c][1] = ctx->q32_cnt[c];
+            continue;
+        }
+        slice_one(ctx->qpref_hi[c], ctx->wpref_hi[c], ctx->shard_rank, ctx->shard_n, ctx->sl_hi[c]);
+        slice_one(ctx->qpref_lo[c], ctx->wpref_lo[c], ctx->shard_rank, ctx->shard_n, ctx->sl_lo[c]);
+    }
+}
+
 // Screened shell-quartet lists for the current tol / FP32 bound.
 pfk_status build_lists(pfk_ctx *ctx)
 {
     const double bound = ctx->precision == PFK_PREC_MIXED ? ctx->fp32_bound : 0.0;
     int maxn = 1;
     for (int x = 0; x < kPairClasses; ++x) maxn = std::max(maxn, (int)ctx->cls_ids[x].size());
-    DevBuf<long long> cnt_hi, cnt_lo, off_hi, off_lo;
+    DevBuf<long long> cnt_hi, cnt_lo, off_hi, off_lo, work_hi, work_lo;
+    PFK_CK(work_hi.alloc(maxn));
+    PFK_CK(work_lo.alloc(maxn));
     PFK_CK(cnt_hi.alloc(maxn));
     PFK_CK(cnt_lo.alloc(maxn));
     PFK_CK(off_hi.alloc(maxn));
@@ -222,6 +266,11 @@ pfk_status build_lists(pfk_ctx *ctx)
             const int cls = quartet_class(x, y);
             const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
             ctx->q_cnt[cls] = ctx->q32_cnt[cls] = 0;
+            ctx->prim_cnt[cls] = 0;
+            ctx->qpref_hi[cls].clear();
+            ctx->qpref_lo[cls].clear();
+            ctx->wpref_hi[cls].clear();
+            ctx->wpref_lo[cls].clear();
             if (nX == 0 || nY == 0) continue;
             PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
                                   cnt_lo.p, ctx->stream));
@@ -262,7 +311,28 @@ pfk_status build_lists(pfk_ctx *ctx)
             PFK_CK(fill_quartets(ctx->d_cls_ids[x].p, nX, ctx->d_cls_ids[y].p, x == y, off_hi.p, cnt_hi.p, off_lo.p,
                                  cnt_lo.p, ctx->d_quart.p + ctx->q_off[cls], ctx->d_quart.p + ctx->q32_off[cls],
                                  ctx->stream));
+            PFK_CK(bra_work(ctx->d_cls_ids[x].p, nX, x == y, cnt_hi.p, cnt_lo.p, ctx->d_cls_kpref[y].p,
+                            ctx->d_pairs.p, work_hi.p, work_lo.p, ctx->stream));
+            std::vector<long long> h(4 * (size_t)nX);
+            PFK_CK(cudaMemcpyAsync(h.data(), cnt_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(h.data() + nX, cnt_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(h.data() + 2 * nX, work_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(h.data() + 3 * nX, work_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaStreamSynchronize(ctx->stream));
+            auto &qh = ctx->qpref_hi[cls], &ql = ctx->qpref_lo[cls], &wh = ctx->wpref_hi[cls], &wl = ctx->wpref_lo[cls];
+            qh.assign(nX + 1, 0);
+            ql.assign(nX + 1, 0);
+            wh.assign(nX + 1, 0);
+            wl.assign(nX + 1, 0);
+            for (int a = 0; a < nX; ++a) {
+                qh[a + 1] = qh[a] + h[a];
+                ql[a + 1] = ql[a] + h[nX + a];
+                wh[a + 1] = wh[a] + h[2 * nX + a];
+                wl[a + 1] = wl[a] + h[3 * nX + a];
+            }
+            ctx->prim_cnt[cls] = wh[nX] + wl[nX];
         }
+    compute_slices(ctx);
     PFK_CK(cudaStreamSynchronize(ctx->stream));
     for (auto &g : ctx->graphs) {   // captured builds refer to the old lists
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -321,6 +391,11 @@ pfk_status schwarz_and_sort(pfk_ctx *ctx)
         PFK_CK(ctx->d_cls_q[x].alloc(v.size()));
         PFK_CK(cudaMemcpyAsync(ctx->d_cls_ids[x].p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
         PFK_CK(cudaMemcpyAsync(ctx->d_cls_q[x].p, q.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<long long> kp(v.size() + 1, 0);
+        for (size_t i = 0; i < v.size(); ++i) kp[i + 1] = kp[i] + ctx->pairs[v[i]].nprim;
+        PFK_CK(ctx->d_cls_kpref[x].alloc(kp.size()));
+        PFK_CK(cudaMemcpyAsync(ctx->d_cls_kpref[x].p, kp.data(), sizeof(long long) * kp.size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
         PFK_CK(cudaStreamSynchronize(ctx->stream));
     }
     return PFK_OK;
@@ -356,11 +431,11 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         PFK_CK(cudaEventCreate(&ev[1]));
     }
     for (int c = 0; c < kQuartetClasses; ++c) {
-        const long long n = ctx->q_cnt[c] + ctx->q32_cnt[c];
-        if (n == 0) continue;
+        const long long nh = ctx->sl_hi[c][1], nl = ctx->sl_lo[c][1];
+        if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
-        if (ctx->q_cnt[c]) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], ctx->q_cnt[c], a, nk, st);
-        if (ctx->q32_cnt[c]) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], ctx->q32_cnt[c], a, nk, st);
+        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c] + ctx->sl_hi[c][0], nh, a, nk, st);
+        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c] + ctx->sl_lo[c][0], nl, a, nk, st);
         PFK_CK(cudaGetLastError());
         if (timed) {
             PFK_CK(cudaEventRecord(ev[1], st));
@@ -515,6 +590,7 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
     for (int x = 0; x < kPairClasses; ++x) {
         ctx->d_cls_ids[x].release();
         ctx->d_cls_q[x].release();
+        ctx->d_cls_kpref[x].release();
     }
     ctx->d_quart.release();
     for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
@@ -720,18 +796,46 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
     return PFK_OK;
 }
 
-pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, double *ms55)
+pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_quartets55, double *ms55)
 {
     if (!ctx) return PFK_ERR_STATE;
     cudaSetDevice(ctx->device);
     if (ms55) {
+        for (int c = 0; c < kQuartetClasses; ++c) ctx->class_ms[c] = 0.f;
         pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, ctx->d_K0.p, nullptr, nullptr,
                                    ctx->stream, true);
         if (s != PFK_OK) return s;
         for (int c = 0; c < kQuartetClasses; ++c) ms55[c] = ctx->class_ms[c];
     }
-    if (quartets55)
-        for (int c = 0; c < kQuartetClasses; ++c) quartets55[c] = ctx->q_cnt[c] + ctx->q32_cnt[c];
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        if (quartets55) quartets55[c] = ctx->q_cnt[c] + ctx->q32_cnt[c];
+        if (prim_quartets55) prim_quartets55[c] = ctx->prim_cnt[c];
+    }
+    return PFK_OK;
+}
+
+pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (nranks < 1 || rank < 0 || rank >= nranks) return ctx->fail(PFK_ERR_INVALID, "need 0 <= rank < nranks");
+    ctx->shard_rank = rank;
+    ctx->shard_n = nranks;
+    compute_slices(ctx);
+    for (auto &g : ctx->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->graphs.clear();
+    return PFK_OK;
+}
+
+pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops)
+{
+    cudaError_t e = measure_fma_peak(device, fp64_tflops, fp32_tflops);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("pfk_measure_fma_peak: ") + cudaGetErrorString(e);
+        return PFK_ERR_CUDA;
+    }
     return PFK_OK;
 }
 

@@ -227,3 +227,85 @@ cudaError_t add(const double *a, const double *b, double *out, long long n, cuda
 }
 
 }  // namespace pfk
+
+namespace pfk {
+
+// Primitive-quartet work of each bra's FP64 and FP32 ket runs:
+// K_bra * (sum of K_ket over the run), from the ket class's nprim prefix.
+__global__ void bra_work_kernel(const int *__restrict__ idX, int nX, int diag, const long long *__restrict__ cnt_hi,
+                                const long long *__restrict__ cnt_lo, const long long *__restrict__ kprefY,
+                                const PairInfo *__restrict__ pairs, long long *work_hi, long long *work_lo)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nX) return;
+    const long long kb = pairs[idX[a]].nprim;
+    const long long s = diag ? a : 0, nh = cnt_hi[a], nl = cnt_lo[a];
+    work_hi[a] = kb * (kprefY[s + nh] - kprefY[s]);
+    work_lo[a] = kb * (kprefY[s + nh + nl] - kprefY[s + nh]);
+}
+
+cudaError_t bra_work(const int *idX, int nX, int diag, const long long *cnt_hi, const long long *cnt_lo,
+                     const long long *kprefY, const PairInfo *pairs, long long *work_hi, long long *work_lo,
+                     cudaStream_t st)
+{
+    if (nX > 0)
+        bra_work_kernel<<<(nX + 127) / 128, 128, 0, st>>>(idX, nX, diag, cnt_hi, cnt_lo, kprefY, pairs, work_hi,
+                                                          work_lo);
+    return cudaGetLastError();
+}
+
+// FMA throughput probe: eight independent dependency chains per thread,
+// all in registers.
+template <typename T>
+__global__ void __launch_bounds__(256) fma_chain_kernel(T *out, int iters, T a, T b)
+{
+    T x0 = T(threadIdx.x) * T(1e-3), x1 = x0 + T(1), x2 = x0 + T(2), x3 = x0 + T(3);
+    T x4 = x0 + T(4), x5 = x0 + T(5), x6 = x0 + T(6), x7 = x0 + T(7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+template <typename T>
+static cudaError_t time_fma(int device, double *tflops)
+{
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 4096;
+    T *out = nullptr;
+    e = cudaMalloc(&out, sizeof(T) * blocks * threads);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fma_chain_kernel<T><<<blocks, threads>>>(out, iters / 8, T(0.9999999), T(1e-7));   // warm-up
+    cudaEventRecord(a);
+    fma_chain_kernel<T><<<blocks, threads>>>(out, iters, T(0.9999999), T(1e-7));
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess) return e;
+    const double flops = 2.0 * 64.0 * (double)iters * blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return cudaGetLastError();
+}
+
+cudaError_t measure_fma_peak(int device, double *fp64, double *fp32)
+{
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess && fp64) e = time_fma<double>(device, fp64);
+    if (e == cudaSuccess && fp32) e = time_fma<float>(device, fp32);
+    return e;
+}
+
+}  // namespace pfk

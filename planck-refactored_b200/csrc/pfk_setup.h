@@ -19,5 +19,9 @@ cudaError_t census(const uint2 *q, long long nq, const PairInfo *pairs, const in
                    cudaStream_t st);
 cudaError_t combine(const double *J, const double *K, double cj, double ck, double *out, int nb, cudaStream_t st);
 cudaError_t add(const double *a, const double *b, double *out, long long n, cudaStream_t st);
+cudaError_t bra_work(const int *idX, int nX, int diag, const long long *cnt_hi, const long long *cnt_lo,
+                     const long long *kprefY, const PairInfo *pairs, long long *work_hi, long long *work_lo,
+                     cudaStream_t st);
+cudaError_t measure_fma_peak(int device, double *fp64, double *fp32);
 
 }  // namespace pfk

@@ -5,7 +5,8 @@ Run in a container where the reference is mounted (default /root/reference):
     python tests/golden/make_fixtures.py [--ref /root/reference]
 
 Writes, next to this script:
-  basis_sets.json         Gaussian94 basis data (exponents, raw contraction
+  ../../planck-refactored_b200/data/basis_sets.json
+                          Gaussian94 basis data (exponents, raw contraction
                           coefficients) for H, C, N, O in the basis sets the
                           tests and benchmarks use, parsed with the same rules
                           as the reference parser (src/basis/gaussian.cpp:54-163:
@@ -107,7 +108,7 @@ def main():
     for name, fname in BASIS_FILES.items():
         data = parse_gbs(open(os.path.join(ref, "basis-sets", fname)).read())
         basis[name] = {el: data[el] for el in ELEMENTS if el in data}
-    with open(os.path.join(HERE, "basis_sets.json"), "w") as f:
+    with open(os.path.join(REPO, "planck-refactored_b200", "data", "basis_sets.json"), "w") as f:
         json.dump({"source": "reference basis-sets/ (Basis Set Exchange data), parsed per gaussian.cpp:54-163",
                    "basis": basis}, f, indent=1)
 
