@@ -214,7 +214,10 @@ def ours_arm(args):
     Pm = density(nb)
     dP = torch.tensor(Pm, device=f"cuda:{local}", dtype=torch.float64)
     dG = torch.zeros_like(dP)
-    stream = torch.cuda.current_stream()
+    # a real (non-default) stream: the graph is captured and replayed on it,
+    # and the timing events are recorded on it
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
 
     def step():
         eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), stream.cuda_stream)

@@ -175,6 +175,8 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
             pi.ABy = ca[1] - cb[1];
             pi.ABz = ca[2] - cb[2];
             const double R2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+            std::vector<PrimPair> pp;
+            pp.reserve(pi.nprim);
             for (int ia = 0; ia < b->nprim[A]; ++ia)
                 for (int ib = 0; ib < b->nprim[B]; ++ib) {
                     const double alpha = b->expo[poff[A] + ia], beta = b->expo[poff[B] + ib];
@@ -190,8 +192,14 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
                     p.PAz = p.Pz - ca[2];
                     p.K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) * b->coef[poff[A] + ia] *
                           b->coef[poff[B] + ib] * b->norm[poff[A] + ia] * b->norm[poff[B] + ib];
-                    ctx->prims.push_back(p);
+                    pp.push_back(p);
                 }
+            std::stable_sort(pp.begin(), pp.end(),
+                             [](const PrimPair &x, const PrimPair &y) { return std::fabs(x.K) > std::fabs(y.K); });
+            pi.nprim_full = (int)pp.size();
+            pi.nprim = 0;
+            while (pi.nprim < pi.nprim_full && std::fabs(pp[pi.nprim].K) >= kPrimPairCut) ++pi.nprim;
+            ctx->prims.insert(ctx->prims.end(), pp.begin(), pp.end());
             ctx->pairs.push_back(pi);
             ctx->pair_pc.push_back(pair_class(b->L[A], b->L[B]));
             ctx->pair_la.push_back(b->L[A]);
@@ -392,7 +400,7 @@ pfk_status schwarz_and_sort(pfk_ctx *ctx)
         PFK_CK(cudaMemcpyAsync(ctx->d_cls_ids[x].p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
         PFK_CK(cudaMemcpyAsync(ctx->d_cls_q[x].p, q.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
         std::vector<long long> kp(v.size() + 1, 0);
-        for (size_t i = 0; i < v.size(); ++i) kp[i + 1] = kp[i] + ctx->pairs[v[i]].nprim;
+        for (size_t i = 0; i < v.size(); ++i) kp[i + 1] = kp[i] + ctx->pairs[v[i]].nprim_full;
         PFK_CK(ctx->d_cls_kpref[x].alloc(kp.size()));
         PFK_CK(cudaMemcpyAsync(ctx->d_cls_kpref[x].p, kp.data(), sizeof(long long) * kp.size(), cudaMemcpyHostToDevice,
                                ctx->stream));

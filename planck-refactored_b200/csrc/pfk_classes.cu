@@ -17,21 +17,30 @@ template <int LA, int LB, int LC, int LD>
 void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, cudaStream_t st)
 {
     using S = ClassShape<LA, LB, LC, LD>;
-    if constexpr (S::N > kRegMaxComponents) {
+    using SS = SplitShape<LA, LB, LC, LD>;
+    using TS = TeamShape<LA, LB, LC, LD>;
+    if constexpr (S::N <= kRegMaxComponents) {
+        if (n <= 0) return;
+        const long long grid = (n + 127) / 128;
+        if (nk == 2) eri_reg_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+        else eri_reg_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+    } else if constexpr (SS::OK) {
         if (n < 0) {  // configure the current device (shared-memory opt-in)
-            using TS = TeamShape<LA, LB, LC, LD>;
+            cudaFuncSetAttribute(eri_split_kernel<LA, LB, LC, LD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::SMEM);
+            cudaFuncSetAttribute(eri_split_kernel<LA, LB, LC, LD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::SMEM);
+            return;
+        }
+        if (n == 0) return;
+        const long long grid = (n + SS::TEAMS - 1) / SS::TEAMS;
+        if (nk == 2) eri_split_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, SS::SMEM, st>>>(q, n, a);
+        else eri_split_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, SS::SMEM, st>>>(q, n, a);
+    } else {
+        if (n < 0) {
             cudaFuncSetAttribute(eri_team_kernel<LA, LB, LC, LD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
             cudaFuncSetAttribute(eri_team_kernel<LA, LB, LC, LD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
             return;
         }
-    }
-    if (n <= 0) return;
-    if constexpr (S::N <= kRegMaxComponents) {
-        const long long grid = (n + 127) / 128;
-        if (nk == 2) eri_reg_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
-        else eri_reg_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
-    } else {
-        using TS = TeamShape<LA, LB, LC, LD>;
+        if (n == 0) return;
         const long long grid = (n + TS::TEAMS - 1) / TS::TEAMS;
         if (nk == 2) eri_team_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);
         else eri_team_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);

@@ -65,13 +65,24 @@ struct __align__(16) PrimPair {
     double K, pad;
 };
 
-// Shell pair a <= b (shell order), oriented so that L(A) >= L(B).
+// Shell pair a <= b (shell order), oriented so that L(A) >= L(B).  Its
+// primitive pairs are stored by decreasing |K|; the first nprim have
+// |K| >= kPrimPairCut and are the ones the Fock build evaluates, all
+// nprim_full of them enter the Schwarz table.
 struct __align__(16) PairInfo {
     int prim_off, nprim;     // range in the PrimPair array
     int bf_a, bf_b;          // first basis function of A and of B
     double ABx, ABy, ABz;    // A - B
     double qmax, qmin;       // max / min of Q(i,j) over the pair's components
+    int nprim_full, pad_;
 };
+
+// Primitive pairs with |K| below this, and primitive quartets with
+// |K_ab K_cd| below kPrimQuartetCut, contribute less than ~1e-16 to any
+// integral (2 sqrt(rho/pi) <= ~1e2 for exponents up to 1e4 and the angular
+// factors stay below ~1e6 where K is not already negligible) and are skipped.
+constexpr double kPrimPairCut = 1e-21;
+constexpr double kPrimQuartetCut = 1e-24;
 
 struct JKArgs {
     const PairInfo *__restrict__ pairs;

@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
         const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
         for (int jp = 0; jp < pk.nprim; ++jp) {
             const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             double u[NR], w[NR];
             rys_roots<NR>(s.T, u, w);
@@ -253,13 +254,13 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Team path (TEAM = 32: one warp per quartet, 4 per block; TEAM = 128: the
-// whole block per quartet).
+// Team path (TEAM = 8: four quartets per warp; TEAM = 32: one warp per
+// quartet; TEAM = 128: the whole block per quartet).
 // ---------------------------------------------------------------------------
 template <int LA, int LB, int LC, int LD>
 struct TeamShape {
     using S = ClassShape<LA, LB, LC, LD>;
-    static constexpr int TEAM = S::N <= 1300 ? 32 : 128;
+    static constexpr int TEAM = S::N <= 400 ? 8 : S::N <= 1300 ? 32 : 128;
     static constexpr int TEAMS = 128 / TEAM;
     static constexpr int KPT = (S::N + TEAM - 1) / TEAM;
     static constexpr int TABLE = S::NR * 3 * S::NI;          // doubles per team
@@ -267,9 +268,9 @@ struct TeamShape {
 };
 
 template <int TEAM>
-__device__ __forceinline__ void team_sync()
+__device__ __forceinline__ void team_sync(unsigned mask)
 {
-    if constexpr (TEAM == 32) __syncwarp();
+    if constexpr (TEAM <= 32) __syncwarp(mask);
     else __syncthreads();
 }
 
@@ -283,9 +284,11 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
     extern __shared__ double smem[];
     const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
     const long long t = (long long)blockIdx.x * TS::TEAMS + team;
-    // TEAM == 32 teams are whole warps and may leave together; the block-wide
-    // team has exactly one quartet per block, so no thread waits on a leaver.
+    // Teams within a warp synchronise only their own lanes, so a team may
+    // leave early; the block-wide team has exactly one quartet per block.
     if (t >= nq) return;
+    const unsigned mask = TEAM >= 32 ? 0xffffffffu
+                                     : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
     double *g = smem + team * TS::TABLE;   // g[r][axis][NI]
 
     const uint2 qd = quartets[t];
@@ -313,6 +316,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
         const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
         for (int jp = 0; jp < pk.nprim; ++jp) {
             const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             for (int task = lane; task < 3 * NR; task += TEAM) {
                 const int r = task / 3, axis = task - 3 * r;
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
                 else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
                 axis_table<LA, LB, LC, LD, double>(C00, D00, B00, B10, B01, AB, CD, scale, g + (r * 3 + axis) * NI);
             }
-            team_sync<TEAM>();
+            team_sync<TEAM>(mask);
 #pragma unroll
             for (int k = 0; k < KPT; ++k) {
                 const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
                     a += g[(r * 3 + 0) * NI + ox] * g[(r * 3 + 1) * NI + oy] * g[(r * 3 + 2) * NI + oz];
                 acc[k] = a;
             }
-            team_sync<TEAM>();
+            team_sync<TEAM>(mask);
         }
     }
 
@@ -390,9 +394,9 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pai
     double acc[NA * NB];
 #pragma unroll
     for (int c = 0; c < NA * NB; ++c) acc[c] = 0.0;
-    for (int ip = 0; ip < pb.nprim; ++ip) {
+    for (int ip = 0; ip < pb.nprim_full; ++ip) {
         const PrimPair p = load_prim(prims, pb.prim_off + ip);
-        for (int jp = 0; jp < pb.nprim; ++jp) {
+        for (int jp = 0; jp < pb.nprim_full; ++jp) {
             const PrimPair q = load_prim(prims, pb.prim_off + jp);
             const QuartetScalars s = quartet_scalars(p, q);
             double u[NR], w[NR];
@@ -424,6 +428,271 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pai
             Qao[(size_t)i * nb + j] = q;
             Qao[(size_t)j * nb + i] = q;
         }
+}
+
+}  // namespace pfk
+
+namespace pfk {
+
+// ---------------------------------------------------------------------------
+// Split path for mid-size classes.  A team of GROUP threads shares one shell
+// quartet: per primitive quartet the 3*NR per-root axis tables are built
+// once (the team's lanes take the (root, axis) tasks) into shared memory;
+// thread g then owns every Cartesian component whose leading index is g --
+// the A component (LEVEL 1) or the (A, B) component pair (LEVEL 2) -- so it
+// needs only the matching slice of each table, which it copies to registers
+// once per root, and accumulates its M components in registers.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int pow2ceil(int x) { return x <= 1 ? 1 : 2 * pow2ceil((x + 1) / 2); }
+
+template <int LA, int LB, int LC, int LD>
+struct SplitShape {
+    using S = ClassShape<LA, LB, LC, LD>;
+    static constexpr int LEVEL = (S::NB * S::NC * S::ND <= 64) ? 1 : 2;
+    static constexpr int GROUP = LEVEL == 1 ? S::NA : S::NA * S::NB;
+    static constexpr int M = S::N / GROUP;                    // components per thread
+    static constexpr int NBT = LEVEL == 1 ? S::NB : 1;        // B components per thread
+    static constexpr int TEAM = pow2ceil(GROUP) < 4 ? 4 : pow2ceil(GROUP);
+    static constexpr int TEAMS = 128 / TEAM;
+    static constexpr int SB = LEVEL == 1 ? (LB + 1) * (LC + 1) * (LD + 1) : (LC + 1) * (LD + 1);
+    static constexpr int TABLE = S::NR * 3 * S::NI;
+    static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
+    static constexpr bool OK = TEAM <= 128 && M <= 64;
+};
+
+template <int TEAM>
+__device__ __forceinline__ void split_sync(unsigned mask, int team)
+{
+    if constexpr (TEAM <= 32) {
+        __syncwarp(mask);
+    } else if constexpr (TEAM == 64) {
+        asm volatile("bar.sync %0, 64;" ::"r"(team + 1) : "memory");
+    } else {
+        __syncthreads();
+    }
+}
+
+// Component norm for a runtime component index (same values as cart_norm).
+template <int L>
+__device__ __forceinline__ double cart_norm_rt(int i)
+{
+    double v = 1.0;
+#pragma unroll
+    for (int c = 0; c < ncart(L); ++c)
+        if (c == i) v = cart_norm(L, c);
+    return v;
+}
+
+template <int L>
+__device__ __forceinline__ int cart_l_axis(int i, int axis)
+{
+    return axis == 0 ? cart_lx(L, i) : axis == 1 ? cart_ly(L, i) : cart_lz(L, i);
+}
+
+template <int LA, int LB, int LC, int LD, int NK>
+__global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
+{
+    using S = ClassShape<LA, LB, LC, LD>;
+    using SS = SplitShape<LA, LB, LC, LD>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
+    constexpr int TEAM = SS::TEAM, LEVEL = SS::LEVEL, NBT = SS::NBT, SB = SS::SB, M = SS::M;
+    extern __shared__ double smem[];
+    const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
+    const long long t = (long long)blockIdx.x * SS::TEAMS + team;
+    if (t >= nq) return;   // whole teams leave together; barriers are per team
+    const unsigned mask = TEAM >= 32 ? 0xffffffffu
+                                     : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
+    double *g = smem + team * SS::TABLE;   // g[r][axis][NI]
+
+    const uint2 qd = quartets[t];
+    const PairInfo pb = args.pairs[qd.x];
+    const PairInfo pk = args.pairs[qd.y];
+    const bool owner = lane < SS::GROUP;
+    const int gi = owner ? lane : 0;
+    const int ia = LEVEL == 1 ? gi : gi / NB;
+    const int ib0 = LEVEL == 1 ? 0 : gi % NB;
+    // slice base of each axis table for this thread's leading indices
+    int base[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const int la = cart_l_axis<LA>(ia, x);
+        base[x] = LEVEL == 1 ? la * SB : (la * (LB + 1) + cart_l_axis<LB>(ib0, x)) * SB;
+    }
+
+    double acc[M];
+#pragma unroll
+    for (int c = 0; c < M; ++c) acc[c] = 0.0;
+
+    for (int ip = 0; ip < pb.nprim; ++ip) {
+        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+        for (int jp = 0; jp < pk.nprim; ++jp) {
+            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
+            const QuartetScalars s = quartet_scalars(p, q);
+            for (int task = lane; task < 3 * NR; task += TEAM) {
+                const int r = task / 3, axis = task - 3 * r;
+                double ur, wr;
+                rys_root_one<NR>(s.T, r, ur, wr);
+                const double B00 = 0.5 * s.rdelta * ur;
+                const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
+                const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
+                double C00, D00, AB, CD, scale = 1.0;
+                if (axis == 0) { C00 = p.PAx + ur * s.WPx; D00 = q.PAx + ur * s.WQx; AB = pb.ABx; CD = pk.ABx; scale = wr * s.pref; }
+                else if (axis == 1) { C00 = p.PAy + ur * s.WPy; D00 = q.PAy + ur * s.WQy; AB = pb.ABy; CD = pk.ABy; }
+                else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
+                axis_table<LA, LB, LC, LD, double>(C00, D00, B00, B10, B01, AB, CD, scale, g + (r * 3 + axis) * NI);
+            }
+            split_sync<TEAM>(mask, team);
+            if (owner) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    double tx[SB], ty[SB], tz[SB];
+#pragma unroll
+                    for (int e = 0; e < SB; ++e) {
+                        tx[e] = g[(r * 3 + 0) * NI + base[0] + e];
+                        ty[e] = g[(r * 3 + 1) * NI + base[1] + e];
+                        tz[e] = g[(r * 3 + 2) * NI + base[2] + e];
+                    }
+#pragma unroll
+                    for (int bl = 0; bl < NBT; ++bl)
+#pragma unroll
+                        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                            for (int id = 0; id < ND; ++id) {
+                                const int c = (bl * NC + ic) * ND + id;
+                                int ox, oy, oz;
+                                if constexpr (LEVEL == 1) {
+                                    ox = (cart_lx(LB, bl) * (LC + 1) + cart_lx(LC, ic)) * (LD + 1) + cart_lx(LD, id);
+                                    oy = (cart_ly(LB, bl) * (LC + 1) + cart_ly(LC, ic)) * (LD + 1) + cart_ly(LD, id);
+                                    oz = (cart_lz(LB, bl) * (LC + 1) + cart_lz(LC, ic)) * (LD + 1) + cart_lz(LD, id);
+                                } else {
+                                    ox = cart_lx(LC, ic) * (LD + 1) + cart_lx(LD, id);
+                                    oy = cart_ly(LC, ic) * (LD + 1) + cart_ly(LD, id);
+                                    oz = cart_lz(LC, ic) * (LD + 1) + cart_lz(LD, id);
+                                }
+                                acc[c] += tx[ox] * ty[oy] * tz[oz];
+                            }
+                }
+            }
+            split_sync<TEAM>(mask, team);
+        }
+    }
+    if (!owner) return;
+
+    // ---- digestion of this thread's components: A index ia, B indices
+    // ib0 .. ib0 + NBT - 1, all C and D ----
+    const int nb = args.nb;
+    const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
+    const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
+    const bool check = pb.qmin * pk.qmin < args.tol;
+    const int i = i0 + ia;
+
+    if (args.eri_out) {
+#pragma unroll
+        for (int bl = 0; bl < NBT; ++bl)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    const int ib = ib0 + bl;
+                    const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao,
+                                                     nb, i, j0 + ib, k0 + ic, l0 + id, args.tol);
+                    if (sw != 0.0) {
+                        const double nrm = cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+                        scatter8(args.eri_out, nb, i, j0 + ib, k0 + ic, l0 + id, acc[(bl * NC + ic) * ND + id] * nrm);
+                    }
+                }
+        return;
+    }
+
+    const double *__restrict__ Pj = args.Pj;
+    double pcd[NC * ND], jcd[NC * ND];
+#pragma unroll
+    for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+        for (int id = 0; id < ND; ++id) {
+            pcd[ic * ND + id] = __ldg(Pj + (size_t)(k0 + ic) * nb + l0 + id);
+            jcd[ic * ND + id] = 0.0;
+        }
+    double jab[NBT], pab[NBT];
+#pragma unroll
+    for (int bl = 0; bl < NBT; ++bl) {
+        jab[bl] = 0.0;
+        pab[bl] = __ldg(Pj + (size_t)i * nb + j0 + ib0 + bl);
+    }
+    // exchange blocks: K(i,k) [NC], K(j,k) [NBT*NC], K(i,l) [ND], K(j,l) [NBT*ND]
+    double kac[NK][NC], kbc[NK][NBT * NC], kad[NK][ND], kbd[NK][NBT * ND];
+    double pac[NK][NC], pbc[NK][NBT * NC], pad_[NK][ND], pbd[NK][NBT * ND];
+#pragma unroll
+    for (int m = 0; m < NK; ++m) {
+        const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic) {
+            kac[m][ic] = 0.0;
+            pac[m][ic] = __ldg(Pk + (size_t)i * nb + k0 + ic);
+        }
+#pragma unroll
+        for (int id = 0; id < ND; ++id) {
+            kad[m][id] = 0.0;
+            pad_[m][id] = __ldg(Pk + (size_t)i * nb + l0 + id);
+        }
+#pragma unroll
+        for (int bl = 0; bl < NBT; ++bl) {
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) {
+                kbc[m][bl * NC + ic] = 0.0;
+                pbc[m][bl * NC + ic] = __ldg(Pk + (size_t)(j0 + ib0 + bl) * nb + k0 + ic);
+            }
+#pragma unroll
+            for (int id = 0; id < ND; ++id) {
+                kbd[m][bl * ND + id] = 0.0;
+                pbd[m][bl * ND + id] = __ldg(Pk + (size_t)(j0 + ib0 + bl) * nb + l0 + id);
+            }
+        }
+    }
+#pragma unroll
+    for (int bl = 0; bl < NBT; ++bl)
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) {
+                const int ib = ib0 + bl;
+                const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao, nb,
+                                                 i, j0 + ib, k0 + ic, l0 + id, args.tol);
+                const double nrm = cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+                const double v = acc[(bl * NC + ic) * ND + id] * (sw * nrm);
+                jab[bl] += v * pcd[ic * ND + id];
+                jcd[ic * ND + id] += v * pab[bl];
+#pragma unroll
+                for (int m = 0; m < NK; ++m) {
+                    kac[m][ic] += v * pbd[m][bl * ND + id];
+                    kbc[m][bl * NC + ic] += v * pad_[m][id];
+                    kad[m][id] += v * pbc[m][bl * NC + ic];
+                    kbd[m][bl * ND + id] += v * pac[m][ic];
+                }
+            }
+#pragma unroll
+    for (int bl = 0; bl < NBT; ++bl) atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, jab[bl]);
+#pragma unroll
+    for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+        for (int id = 0; id < ND; ++id) atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, jcd[ic * ND + id]);
+#pragma unroll
+    for (int m = 0; m < NK; ++m) {
+        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+        if (!Kacc) continue;
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)i * nb + k0 + ic, kac[m][ic]);
+#pragma unroll
+        for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)i * nb + l0 + id, kad[m][id]);
+#pragma unroll
+        for (int bl = 0; bl < NBT; ++bl) {
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(j0 + ib0 + bl) * nb + k0 + ic, kbc[m][bl * NC + ic]);
+#pragma unroll
+            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(j0 + ib0 + bl) * nb + l0 + id, kbd[m][bl * ND + id]);
+        }
+    }
 }
 
 }  // namespace pfk

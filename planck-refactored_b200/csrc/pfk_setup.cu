@@ -231,14 +231,15 @@ cudaError_t add(const double *a, const double *b, double *out, long long n, cuda
 namespace pfk {
 
 // Primitive-quartet work of each bra's FP64 and FP32 ket runs:
-// K_bra * (sum of K_ket over the run), from the ket class's nprim prefix.
+// K_bra * (sum of K_ket over the run) with all primitives counted (the
+// algorithmic yardstick), from the ket class's nprim_full prefix.
 __global__ void bra_work_kernel(const int *__restrict__ idX, int nX, int diag, const long long *__restrict__ cnt_hi,
                                 const long long *__restrict__ cnt_lo, const long long *__restrict__ kprefY,
                                 const PairInfo *__restrict__ pairs, long long *work_hi, long long *work_lo)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nX) return;
-    const long long kb = pairs[idX[a]].nprim;
+    const long long kb = pairs[idX[a]].nprim_full;
     const long long s = diag ? a : 0, nh = cnt_hi[a], nl = cnt_lo[a];
     work_hi[a] = kb * (kprefY[s + nh] - kprefY[s]);
     work_lo[a] = kb * (kprefY[s + nh + nl] - kprefY[s + nh]);
