@@ -134,11 +134,12 @@ pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_
                            double *ms55);
 
 /* Restrict every later build of this context to shard `rank` of `nranks`:
- * each class's screened quartet list is cut into nranks contiguous slices
- * of equal primitive-quartet work and only slice `rank` is evaluated, so the
- * partial G (or J, K) of all ranks sum to the full result.  nranks = 1
- * restores the whole list.  Used by one-process-per-GPU runs, which sum the
- * partial matrices with one all-reduce. */
+ * of each class's screened quartet list (ordered by primitive loop length)
+ * only every nranks-th quartet starting at `rank` is evaluated, so the
+ * shards carry equal mixes of work and the partial G (or J, K) of all ranks
+ * sum to the full result.  nranks = 1 restores the whole list.  Used by
+ * one-process-per-GPU runs, which sum the partial matrices with one
+ * all-reduce. */
 pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
 
 /* Measurement helper: sustained FP64 and FP32 fused-multiply-add throughput

@@ -32,8 +32,14 @@ DEPS = {
 }
 
 
+# Class ranges per translation unit (class c = X(X+1)/2 + Y for bra pair
+# class X >= ket pair class Y): one unit per f-bra class, grouped below.
+CLASS_UNITS = [(0, 6), (6, 10), (10, 15), (15, 18), (18, 21)] + [(c, c + 1) for c in range(21, 55)]
+
+
 def _units():
-    units = [("pfk_classes.cu", f"classes_{x}.o", [f"-DPFK_BRA_CLASS={x}"]) for x in range(9, -1, -1)]
+    units = [("pfk_classes.cu", f"classes_{b}_{e}.o", [f"-DPFK_CLASS_BEGIN={b}", f"-DPFK_CLASS_END={e}"])
+             for b, e in reversed(CLASS_UNITS)]
     units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", [])]
     return units
 

@@ -14,6 +14,10 @@
 
 using namespace pfk;
 
+namespace pfk {
+ClassLauncher g_class_launchers[kQuartetClasses];   // constant-initialised; filled by the class units
+}
+
 namespace {
 
 thread_local std::string g_last_error;   // for failures without a context
@@ -71,13 +75,8 @@ struct pfk_ctx {
     DevBuf<double> d_cls_q[kPairClasses];
     DevBuf<long long> d_cls_kpref[kPairClasses];   // prefix of nprim over the sorted class list
 
-    // per quartet class, per bra: prefix of quartet counts and of primitive
-    // work for the FP64 ("hi") and FP32 ("lo") lists (size nX + 1)
-    std::vector<long long> qpref_hi[kQuartetClasses], qpref_lo[kQuartetClasses];
-    std::vector<long long> wpref_hi[kQuartetClasses], wpref_lo[kQuartetClasses];
-    long long prim_cnt[kQuartetClasses] = {};
-    int shard_rank = 0, shard_n = 1;
-    long long sl_hi[kQuartetClasses][2] = {}, sl_lo[kQuartetClasses][2] = {};   // [begin, count) of this shard
+    long long prim_cnt[kQuartetClasses] = {};   // primitive quartets (all primitives), per class
+    int shard_rank = 0, shard_n = 1;             // builds evaluate every shard_n-th quartet
 
     double tol = 1e-10, fp32_bound = 1e-8;
     int engine = PFK_ENGINE_OS, precision = PFK_PREC_FP64;
@@ -184,6 +183,7 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
                     PrimPair p{};
                     p.zeta = zeta;
                     p.inv_zeta = iz;
+                    p.sqrt_zeta = std::sqrt(zeta);
                     p.Px = (alpha * ca[0] + beta * cb[0]) * iz;
                     p.Py = (alpha * ca[1] + beta * cb[1]) * iz;
                     p.Pz = (alpha * ca[2] + beta * cb[2]) * iz;
@@ -216,39 +216,6 @@ pfk_status upload_pairs(pfk_ctx *ctx)
     return PFK_OK;
 }
 
-// This shard's slice of each class list: bra boundaries splitting the
-// primitive work into shard_n equal parts.
-void slice_one(const std::vector<long long> &qp, const std::vector<long long> &wp, int r, int n, long long out[2])
-{
-    out[0] = out[1] = 0;
-    if (qp.empty()) return;
-    const long long W = wp.back();
-    auto bound = [&](int k) -> size_t {
-        if (k <= 0) return 0;
-        if (k >= n) return wp.size() - 1;
-        const long long t = (long long)((double)W * k / n);
-        return (size_t)(std::lower_bound(wp.begin(), wp.end(), t) - wp.begin());
-    };
-    const size_t a0 = bound(r), a1 = std::max(a0, bound(r + 1));
-    out[0] = qp[a0];
-    out[1] = qp[a1] - qp[a0];
-}
-
-void compute_slices(pfk_ctx *ctx)
-{
-    for (int c = 0; c < kQuartetClasses; ++c) {
-        if (ctx->shard_n <= 1) {
-            ctx->sl_hi[c][0] = 0;
-            ctx->sl_hi[c][1] = ctx->q_cnt[c];
-            ctx->sl_lo[c][0] = 0;
-            ctx->sl_lo[c][1] = ctx->q32_cnt[c];
-            continue;
-        }
-        slice_one(ctx->qpref_hi[c], ctx->wpref_hi[c], ctx->shard_rank, ctx->shard_n, ctx->sl_hi[c]);
-        slice_one(ctx->qpref_lo[c], ctx->wpref_lo[c], ctx->shard_rank, ctx->shard_n, ctx->sl_lo[c]);
-    }
-}
-
 // Screened shell-quartet lists for the current tol / FP32 bound.
 pfk_status build_lists(pfk_ctx *ctx)
 {
@@ -275,10 +242,6 @@ pfk_status build_lists(pfk_ctx *ctx)
             const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
             ctx->q_cnt[cls] = ctx->q32_cnt[cls] = 0;
             ctx->prim_cnt[cls] = 0;
-            ctx->qpref_hi[cls].clear();
-            ctx->qpref_lo[cls].clear();
-            ctx->wpref_hi[cls].clear();
-            ctx->wpref_lo[cls].clear();
             if (nX == 0 || nY == 0) continue;
             PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
                                   cnt_lo.p, ctx->stream));
@@ -321,26 +284,36 @@ pfk_status build_lists(pfk_ctx *ctx)
                                  ctx->stream));
             PFK_CK(bra_work(ctx->d_cls_ids[x].p, nX, x == y, cnt_hi.p, cnt_lo.p, ctx->d_cls_kpref[y].p,
                             ctx->d_pairs.p, work_hi.p, work_lo.p, ctx->stream));
-            std::vector<long long> h(4 * (size_t)nX);
-            PFK_CK(cudaMemcpyAsync(h.data(), cnt_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
-            PFK_CK(cudaMemcpyAsync(h.data() + nX, cnt_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
-            PFK_CK(cudaMemcpyAsync(h.data() + 2 * nX, work_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
-            PFK_CK(cudaMemcpyAsync(h.data() + 3 * nX, work_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            std::vector<long long> h(2 * (size_t)nX);
+            PFK_CK(cudaMemcpyAsync(h.data(), work_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
+            PFK_CK(cudaMemcpyAsync(h.data() + nX, work_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
             PFK_CK(cudaStreamSynchronize(ctx->stream));
-            auto &qh = ctx->qpref_hi[cls], &ql = ctx->qpref_lo[cls], &wh = ctx->wpref_hi[cls], &wl = ctx->wpref_lo[cls];
-            qh.assign(nX + 1, 0);
-            ql.assign(nX + 1, 0);
-            wh.assign(nX + 1, 0);
-            wl.assign(nX + 1, 0);
-            for (int a = 0; a < nX; ++a) {
-                qh[a + 1] = qh[a] + h[a];
-                ql[a + 1] = ql[a] + h[nX + a];
-                wh[a + 1] = wh[a] + h[2 * nX + a];
-                wl[a + 1] = wl[a] + h[3 * nX + a];
-            }
-            ctx->prim_cnt[cls] = wh[nX] + wl[nX];
+            long long w = 0;
+            for (size_t a = 0; a < h.size(); ++a) w += h[a];
+            ctx->prim_cnt[cls] = w;
         }
-    compute_slices(ctx);
+    // order each list by its primitive loop lengths (stable: bra-major within a key)
+    long long maxseg = 1;
+    for (int c = 0; c < kQuartetClasses; ++c) maxseg = std::max(maxseg, std::max(ctx->q_cnt[c], ctx->q32_cnt[c]));
+    {
+        DevBuf<unsigned> ka, kb;
+        DevBuf<uint2> vb;
+        PFK_CK(ka.alloc(maxseg));
+        PFK_CK(kb.alloc(maxseg));
+        PFK_CK(vb.alloc(maxseg));
+        size_t sort_bytes = 0;
+        PFK_CK(sort_quartets(ctx->d_quart.p, maxseg, ctx->d_pairs.p, ka.p, kb.p, vb.p, nullptr, sort_bytes, ctx->stream));
+        DevBuf<char> st;
+        PFK_CK(st.alloc(sort_bytes + 16));
+        for (int c = 0; c < kQuartetClasses; ++c) {
+            size_t b1 = sort_bytes, b2 = sort_bytes;
+            PFK_CK(sort_quartets(ctx->d_quart.p + ctx->q_off[c], ctx->q_cnt[c], ctx->d_pairs.p, ka.p, kb.p, vb.p, st.p,
+                                 b1, ctx->stream));
+            PFK_CK(sort_quartets(ctx->d_quart.p + ctx->q32_off[c], ctx->q32_cnt[c], ctx->d_pairs.p, ka.p, kb.p, vb.p,
+                                 st.p, b2, ctx->stream));
+        }
+        PFK_CK(cudaStreamSynchronize(ctx->stream));
+    }
     PFK_CK(cudaStreamSynchronize(ctx->stream));
     for (auto &g : ctx->graphs) {   // captured builds refer to the old lists
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -433,17 +406,22 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
     a.eri_out = eri_out;
     a.tol = ctx->tol;
     a.nb = ctx->nb;
+    a.qstride = ctx->shard_n;
+    a.qoffset = ctx->shard_rank;
+    auto local = [&](long long n) -> long long {
+        return n > ctx->shard_rank ? (n - ctx->shard_rank + ctx->shard_n - 1) / ctx->shard_n : 0;
+    };
     cudaEvent_t ev[2] = {nullptr, nullptr};
     if (timed) {
         PFK_CK(cudaEventCreate(&ev[0]));
         PFK_CK(cudaEventCreate(&ev[1]));
     }
     for (int c = 0; c < kQuartetClasses; ++c) {
-        const long long nh = ctx->sl_hi[c][1], nl = ctx->sl_lo[c][1];
+        const long long nh = local(ctx->q_cnt[c]), nl = local(ctx->q32_cnt[c]);
         if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
-        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c] + ctx->sl_hi[c][0], nh, a, nk, st);
-        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c] + ctx->sl_lo[c][0], nl, a, nk, st);
+        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, st);
+        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, st);
         PFK_CK(cudaGetLastError());
         if (timed) {
             PFK_CK(cudaEventRecord(ev[1], st));
@@ -553,16 +531,13 @@ pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
         if (e != cudaSuccess) return bail(ctx->cuda_fail("pair tables", e));
         pfk_status s = upload_pairs(ctx);
         if (s != PFK_OK) return bail(s);
-        register_bra_class_0(ctx->launch);
-        register_bra_class_1(ctx->launch);
-        register_bra_class_2(ctx->launch);
-        register_bra_class_3(ctx->launch);
-        register_bra_class_4(ctx->launch);
-        register_bra_class_5(ctx->launch);
-        register_bra_class_6(ctx->launch);
-        register_bra_class_7(ctx->launch);
-        register_bra_class_8(ctx->launch);
-        register_bra_class_9(ctx->launch);
+        for (int c = 0; c < kQuartetClasses; ++c) {
+            if (!g_class_launchers[c]) {
+                ctx->err = "class kernel table incomplete (library built without every class unit)";
+                return bail(PFK_ERR_STATE);
+            }
+            ctx->launch[c] = g_class_launchers[c];
+        }
         JKArgs none{};
         for (int c = 0; c < kQuartetClasses; ++c) ctx->launch[c](nullptr, -1, none, 1, ctx->stream);
         e = cudaGetLastError();
@@ -828,7 +803,6 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
     if (nranks < 1 || rank < 0 || rank >= nranks) return ctx->fail(PFK_ERR_INVALID, "need 0 <= rank < nranks");
     ctx->shard_rank = rank;
     ctx->shard_n = nranks;
-    compute_slices(ctx);
     for (auto &g : ctx->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         if (g.graph) cudaGraphDestroy(g.graph);

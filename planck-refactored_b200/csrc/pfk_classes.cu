@@ -1,11 +1,11 @@
-// pfk_classes.cu -- launchers of the quartet-class kernels whose bra pair
-// class is PFK_BRA_CLASS (compiled once per bra class, 0..9, so the 55
-// class instantiations build in parallel).
+// pfk_classes.cu -- launchers of quartet classes PFK_CLASS_BEGIN ..
+// PFK_CLASS_END - 1 (the build compiles this file once per class range so the
+// 55 class instantiations build in parallel).
 #include "pfk_internal.h"
 #include "pfk_kernels.cuh"
 
-#ifndef PFK_BRA_CLASS
-#error "PFK_BRA_CLASS must be defined (0..9)"
+#if !defined(PFK_CLASS_BEGIN) || !defined(PFK_CLASS_END)
+#error "PFK_CLASS_BEGIN and PFK_CLASS_END must be defined (0 <= begin < end <= 55)"
 #endif
 
 namespace pfk {
@@ -47,23 +47,28 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, cudaStre
     }
 }
 
-template <int X, int Y>
-void reg_one(ClassLauncher *table)
+// class index -> (bra pair class, ket pair class)
+constexpr int cls_bra(int c)
 {
-    table[quartet_class(X, Y)] = &launch_class<pc_la(X), pc_lb(X), pc_la(Y), pc_lb(Y)>;
-    if constexpr (Y > 0) reg_one<X, Y - 1>(table);
+    int x = 0;
+    while ((x + 1) * (x + 2) / 2 <= c) ++x;
+    return x;
 }
+constexpr int cls_ket(int c) { return c - cls_bra(c) * (cls_bra(c) + 1) / 2; }
+
+template <int C>
+void reg_range(ClassLauncher *table)
+{
+    constexpr int X = cls_bra(C), Y = cls_ket(C);
+    table[C] = &launch_class<pc_la(X), pc_lb(X), pc_la(Y), pc_lb(Y)>;
+    if constexpr (C + 1 < PFK_CLASS_END) reg_range<C + 1>(table);
+}
+
+// Runs at library load: puts this unit's launchers into the shared table.
+struct Registrar {
+    Registrar() { reg_range<PFK_CLASS_BEGIN>(g_class_launchers); }
+};
+const Registrar registrar;
 
 }  // namespace
-
-}  // namespace pfk
-
-#define PFK_CAT2(a, b) a##b
-#define PFK_CAT(a, b) PFK_CAT2(a, b)
-
-namespace pfk {
-void PFK_CAT(register_bra_class_, PFK_BRA_CLASS)(ClassLauncher *table)
-{
-    reg_one<PFK_BRA_CLASS, PFK_BRA_CLASS>(table);
-}
 }  // namespace pfk

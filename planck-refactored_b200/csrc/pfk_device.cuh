@@ -62,7 +62,7 @@ struct __align__(16) PrimPair {
     double zeta, inv_zeta;
     double Px, Py, Pz;
     double PAx, PAy, PAz;   // P - A (A = first centre of the oriented pair)
-    double K, pad;
+    double K, sqrt_zeta;
 };
 
 // Shell pair a <= b (shell order), oriented so that L(A) >= L(B).  Its
@@ -97,6 +97,9 @@ struct JKArgs {
     double *eri_out;                    // dense tensor mode (nb^4) when non-null
     double tol;
     int nb;
+    // this launch evaluates quartets[t * qstride + qoffset], t < nq (one
+    // shard of a list split across GPUs; 1 and 0 for the whole list)
+    int qstride, qoffset;
 };
 
 // ---------------------------------------------------------------------------
@@ -106,17 +109,26 @@ struct JKArgs {
 #define PFK_RYS_TABLE_STORAGE static __device__ const
 #include "rys_table_data.inc"
 
-__device__ __forceinline__ double clenshaw15(const double *__restrict__ c, double x)
+// Clenshaw evaluation of one root's u and w series together: c holds the
+// DEG+1 coefficient pairs (u_k, w_k), read as 16-byte loads.
+__device__ __forceinline__ void clenshaw_pair(const double *__restrict__ c, double x, double &u, double &w)
 {
-    double b1 = 0.0, b2 = 0.0;
+    const double2 *c2 = reinterpret_cast<const double2 *>(c);
+    double bu1 = 0.0, bu2 = 0.0, bw1 = 0.0, bw2 = 0.0;
     const double x2 = 2.0 * x;
 #pragma unroll
     for (int k = PFK_RYS_DEG; k >= 1; --k) {
-        const double t = fma(x2, b1, __ldg(c + k) - b2);
-        b2 = b1;
-        b1 = t;
+        const double2 ck = __ldg(c2 + k);
+        const double tu = fma(x2, bu1, ck.x - bu2);
+        const double tw = fma(x2, bw1, ck.y - bw2);
+        bu2 = bu1;
+        bu1 = tu;
+        bw2 = bw1;
+        bw1 = tw;
     }
-    return fma(x, b1, __ldg(c) - b2);
+    const double2 c0 = __ldg(c2);
+    u = fma(x, bu1, c0.x - bu2);
+    w = fma(x, bw1, c0.y - bw2);
 }
 
 // All NR roots u_r = t_r^2 and weights of the measure exp(-T u) u^-1/2 / 2 du.
@@ -128,10 +140,7 @@ __device__ __forceinline__ void rys_roots(double T, double *u, double *w)
         const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
         const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            u[r] = clenshaw15(base + r * (PFK_RYS_DEG + 1), x);
-            w[r] = clenshaw15(base + (NR + r) * (PFK_RYS_DEG + 1), x);
-        }
+        for (int r = 0; r < NR; ++r) clenshaw_pair(base + r * 2 * (PFK_RYS_DEG + 1), x, u[r], w[r]);
     } else {
         const double iT = 1.0 / T;
         const double isT = sqrt(iT);
@@ -150,8 +159,7 @@ __device__ __forceinline__ void rys_root_one(double T, int r, double &u, double 
         const int iv = (int)(T * (1.0 / PFK_RYS_H));
         const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
         const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
-        u = clenshaw15(base + r * (PFK_RYS_DEG + 1), x);
-        w = clenshaw15(base + (NR + r) * (PFK_RYS_DEG + 1), x);
+        clenshaw_pair(base + r * 2 * (PFK_RYS_DEG + 1), x, u, w);
     } else {
         const double iT = 1.0 / T;
         u = kRysAsymU[NR][r] * iT;
@@ -228,12 +236,13 @@ __device__ __forceinline__ QuartetScalars quartet_scalars(const PrimPair &p, con
 {
     QuartetScalars s;
     const double delta = p.zeta + q.zeta;
-    s.rdelta = 1.0 / delta;
+    const double rs = rsqrt(delta);          // 1/sqrt(zeta + eta)
+    s.rdelta = rs * rs;
     s.rho = p.zeta * q.zeta * s.rdelta;
     const double PQx = p.Px - q.Px, PQy = p.Py - q.Py, PQz = p.Pz - q.Pz;
     s.T = s.rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-    // 2 sqrt(rho / pi) K_ab K_cd  (rys.cpp:415)
-    s.pref = 1.1283791670955125739 * sqrt(s.rho) * p.K * q.K;
+    // 2 sqrt(rho / pi) K_ab K_cd  (rys.cpp:415), sqrt(rho) = sqrt(zeta) sqrt(eta) / sqrt(delta)
+    s.pref = 1.1283791670955125739 * (p.sqrt_zeta * q.sqrt_zeta * rs) * (p.K * q.K);
     s.zinv = p.inv_zeta;
     s.einv = q.inv_zeta;
     const double fp = -q.zeta * s.rdelta, fq = p.zeta * s.rdelta;  // W-P = fp PQ, W-Q = fq PQ
@@ -248,7 +257,7 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
     const double2 x0 = __ldg(v), x1 = __ldg(v + 1), x2 = __ldg(v + 2), x3 = __ldg(v + 3), x4 = __ldg(v + 4);
     PrimPair p;
     p.zeta = x0.x; p.inv_zeta = x0.y; p.Px = x1.x; p.Py = x1.y; p.Pz = x2.x;
-    p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.K = x4.x; p.pad = 0.0;
+    p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.K = x4.x; p.sqrt_zeta = x4.y;
     return p;
 }
 

@@ -17,17 +17,9 @@ __host__ __device__ constexpr int quartet_class(int bra_pc, int ket_pc) { return
 // One launcher per quartet class.  nk = number of exchange densities (1 or 2).
 using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, cudaStream_t st);
 
-// pfk_classes.cu, compiled once per bra class; a launcher called with
+// Launchers of the 55 classes, filled at library load by the pfk_classes.cu
+// units (each compiled for a range of classes).  A launcher called with
 // n < 0 only configures the current device for its kernels.
-void register_bra_class_0(ClassLauncher *table);
-void register_bra_class_1(ClassLauncher *table);
-void register_bra_class_2(ClassLauncher *table);
-void register_bra_class_3(ClassLauncher *table);
-void register_bra_class_4(ClassLauncher *table);
-void register_bra_class_5(ClassLauncher *table);
-void register_bra_class_6(ClassLauncher *table);
-void register_bra_class_7(ClassLauncher *table);
-void register_bra_class_8(ClassLauncher *table);
-void register_bra_class_9(ClassLauncher *table);
+extern ClassLauncher g_class_launchers[kQuartetClasses];
 
 }  // namespace pfk

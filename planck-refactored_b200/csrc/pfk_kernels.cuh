@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nq) return;
-    const uint2 qd = quartets[t];
+    const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
 
@@ -84,11 +84,13 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
 #pragma unroll
     for (int c = 0; c < S::N; ++c) acc[c] = 0.0;
 
-    for (int ip = 0; ip < pb.nprim; ++ip) {
-        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-        for (int jp = 0; jp < pk.nprim; ++jp) {
-            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
+    // ket primitives outer: a warp's lanes usually share the bra pair, so the
+    // inner loads of bra primitives are broadcasts
+    for (int jp = 0; jp < pk.nprim; ++jp) {
+        const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        for (int ip = 0; ip < pb.nprim; ++ip) {
+            const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             double u[NR], w[NR];
             rys_roots<NR>(s.T, u, w);
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
                                      : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
     double *g = smem + team * TS::TABLE;   // g[r][axis][NI]
 
-    const uint2 qd = quartets[t];
+    const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
 
@@ -312,11 +314,13 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
         }
     }
 
-    for (int ip = 0; ip < pb.nprim; ++ip) {
-        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-        for (int jp = 0; jp < pk.nprim; ++jp) {
-            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
+    // ket primitives outer: a warp's lanes usually share the bra pair, so the
+    // inner loads of bra primitives are broadcasts
+    for (int jp = 0; jp < pk.nprim; ++jp) {
+        const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        for (int ip = 0; ip < pb.nprim; ++ip) {
+            const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             for (int task = lane; task < 3 * NR; task += TEAM) {
                 const int r = task / 3, axis = task - 3 * r;
@@ -504,7 +508,7 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
                                      : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
     double *g = smem + team * SS::TABLE;   // g[r][axis][NI]
 
-    const uint2 qd = quartets[t];
+    const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
     const bool owner = lane < SS::GROUP;
@@ -523,11 +527,13 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
 #pragma unroll
     for (int c = 0; c < M; ++c) acc[c] = 0.0;
 
-    for (int ip = 0; ip < pb.nprim; ++ip) {
-        const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-        for (int jp = 0; jp < pk.nprim; ++jp) {
-            const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // kets sorted by |K|
+    // ket primitives outer: a warp's lanes usually share the bra pair, so the
+    // inner loads of bra primitives are broadcasts
+    for (int jp = 0; jp < pk.nprim; ++jp) {
+        const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        for (int ip = 0; ip < pb.nprim; ++ip) {
+            const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
+            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             for (int task = lane; task < 3 * NR; task += TEAM) {
                 const int r = task / 3, axis = task - 3 * r;

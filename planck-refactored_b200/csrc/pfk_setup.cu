@@ -310,3 +310,39 @@ cudaError_t measure_fma_peak(int device, double *fp64, double *fp32)
 }
 
 }  // namespace pfk
+
+#include <cub/device/device_radix_sort.cuh>
+
+namespace pfk {
+
+// Sort key of a shell quartet: (evaluated bra primitives, evaluated ket
+// primitives), so that a warp's lanes run the same primitive loop lengths.
+__global__ void quartet_key_kernel(const uint2 *__restrict__ q, long long n, const PairInfo *__restrict__ pairs,
+                                   unsigned *keys)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint2 v = q[t];
+    keys[t] = (unsigned)pairs[v.x].nprim * 4096u + (unsigned)pairs[v.y].nprim;
+}
+
+// Stable sort of one list segment by its key; tmp buffers sized by the caller
+// (keys_a/keys_b: n unsigned, vals_b: n uint2, temp: temp_bytes).
+cudaError_t sort_quartets(uint2 *q, long long n, const PairInfo *pairs, unsigned *keys_a, unsigned *keys_b,
+                          uint2 *vals_b, void *temp, size_t &temp_bytes, cudaStream_t st)
+{
+    if (!temp) {
+        return cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys_a, keys_b,
+                                               reinterpret_cast<unsigned long long *>(q),
+                                               reinterpret_cast<unsigned long long *>(vals_b), n, 0, 24, st);
+    }
+    if (n <= 1) return cudaSuccess;
+    quartet_key_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q, n, pairs, keys_a);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_a, keys_b,
+                                                    reinterpret_cast<unsigned long long *>(q),
+                                                    reinterpret_cast<unsigned long long *>(vals_b), n, 0, 24, st);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(q, vals_b, sizeof(uint2) * n, cudaMemcpyDeviceToDevice, st);
+}
+
+}  // namespace pfk

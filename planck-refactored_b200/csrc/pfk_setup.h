@@ -23,5 +23,7 @@ cudaError_t bra_work(const int *idX, int nX, int diag, const long long *cnt_hi, 
                      const long long *kprefY, const PairInfo *pairs, long long *work_hi, long long *work_lo,
                      cudaStream_t st);
 cudaError_t measure_fma_peak(int device, double *fp64, double *fp32);
+cudaError_t sort_quartets(uint2 *q, long long n, const PairInfo *pairs, unsigned *keys_a, unsigned *keys_b,
+                          uint2 *vals_b, void *temp, size_t &temp_bytes, cudaStream_t st);
 
 }  // namespace pfk

@@ -23,7 +23,9 @@ Output: csrc/rys_table_data.inc (C initialisers, committed; regenerate with
 `python gen_rys_table.py`).  The includer defines PFK_RYS_CONST_STORAGE and
 PFK_RYS_TABLE_STORAGE (e.g. `static __constant__ const` and
 `static __device__ const`) so every translation unit gets statically
-initialised device copies.  The script also prints the measured maximum
+initialised device copies.  Layout: per n, per interval, per root r, the
+DEG+1 Chebyshev coefficients of u_r and w_r interleaved (u_0, w_0, u_1, w_1,
+...), so the device reads one (u, w) coefficient pair per 16-byte load.  The script also prints the measured maximum
 interpolation error at random T against fresh 80-digit evaluations.
 """
 import multiprocessing as mproc
@@ -195,12 +197,13 @@ def main():
             off += layout[n - 1] * 2 * n * N
         f.write("PFK_RYS_CONST_STORAGE int kRysOffset[PFK_RYS_NMAX + 1] = {" + ", ".join(str(o) for o in offs) + "};\n")
         f.write(f"#define PFK_RYS_TABLE_SIZE {off}\n")
-        f.write("PFK_RYS_TABLE_STORAGE double kRysCheb[PFK_RYS_TABLE_SIZE] = {\n")
+        f.write("PFK_RYS_TABLE_STORAGE double __align__(16) kRysCheb[PFK_RYS_TABLE_SIZE] = {\n")
         for n in range(1, NMAX + 1):
-            f.write(f"// n = {n}: {layout[n-1]} intervals x {2*n} values x {N} coefficients\n")
+            f.write(f"// n = {n}: {layout[n-1]} intervals x {n} roots x {N} coefficients x (u, w)\n")
             for i in range(layout[n - 1]):
-                for v in range(2 * n):
-                    f.write(",".join(f"{c:.17g}" for c in tables[n][i][v]) + ",\n")
+                for r in range(n):
+                    f.write(",".join(f"{cu:.17g},{cw:.17g}" for cu, cw in
+                                     zip(tables[n][i][r], tables[n][i][n + r])) + ",\n")
         f.write("};\n")
         # large-T limit constants: x_i^2 and W_i for each n
         f.write("PFK_RYS_CONST_STORAGE double kRysAsymU[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")

@@ -155,8 +155,9 @@ def test_device_rys_table_reproduces_boys_moments():
                 iv = int(T / 2.0)
                 x = (T - iv * 2.0) - 1.0
                 base = off[n] + iv * 2 * n * 15
-                u = np.array([_cheb(cheb[base + r * 15: base + r * 15 + 15], x) for r in range(n)])
-                w = np.array([_cheb(cheb[base + (n + r) * 15: base + (n + r) * 15 + 15], x) for r in range(n)])
+                # per root: 15 (u_k, w_k) coefficient pairs
+                u = np.array([_cheb(cheb[base + r * 30: base + r * 30 + 30: 2], x) for r in range(n)])
+                w = np.array([_cheb(cheb[base + r * 30 + 1: base + r * 30 + 30: 2], x) for r in range(n)])
             else:
                 u = np.array(au[n - 1]) / T
                 w = np.array(aw[n - 1]) / np.sqrt(T)
