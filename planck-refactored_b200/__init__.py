@@ -16,7 +16,7 @@ import os
 
 import numpy as np
 
-from . import workloads  # noqa: F401
+from . import shard, workloads  # noqa: F401
 from .basis import (ANGSTROM_TO_BOHR, Molecule, cartesian_order, component_norm,  # noqa: F401
                     read_gbs_basis, shells_for)
 

@@ -109,16 +109,18 @@ struct JKArgs {
 #define PFK_RYS_TABLE_STORAGE static __device__ const
 #include "rys_table_data.inc"
 
-// Clenshaw evaluation of one root's u and w series together: c holds the
-// DEG+1 coefficient pairs (u_k, w_k), read as 16-byte loads.
-__device__ __forceinline__ void clenshaw_pair(const double *__restrict__ c, double x, double &u, double &w)
+// Clenshaw evaluation of one root's u and w series together.  c points at
+// the (u_0, w_0) pair of this root and interval; consecutive degrees are
+// `stride` pairs apart (table layout: [k][root][interval][u, w]).
+__device__ __forceinline__ void clenshaw_pair(const double *__restrict__ c, int stride, double x, double &u,
+                                              double &w)
 {
     const double2 *c2 = reinterpret_cast<const double2 *>(c);
     double bu1 = 0.0, bu2 = 0.0, bw1 = 0.0, bw2 = 0.0;
     const double x2 = 2.0 * x;
 #pragma unroll
     for (int k = PFK_RYS_DEG; k >= 1; --k) {
-        const double2 ck = __ldg(c2 + k);
+        const double2 ck = __ldg(c2 + k * stride);
         const double tu = fma(x2, bu1, ck.x - bu2);
         const double tw = fma(x2, bw1, ck.y - bw2);
         bu2 = bu1;
@@ -138,9 +140,10 @@ __device__ __forceinline__ void rys_roots(double T, double *u, double *w)
     if (T < kRysTmax[NR]) {
         const int iv = (int)(T * (1.0 / PFK_RYS_H));
         const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
-        const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
+        const int nint = kRysNint[NR];
+        const double *base = kRysCheb + kRysOffset[NR] + 2 * iv;
 #pragma unroll
-        for (int r = 0; r < NR; ++r) clenshaw_pair(base + r * 2 * (PFK_RYS_DEG + 1), x, u[r], w[r]);
+        for (int r = 0; r < NR; ++r) clenshaw_pair(base + 2 * r * nint, NR * nint, x, u[r], w[r]);
     } else {
         const double iT = 1.0 / T;
         const double isT = sqrt(iT);
@@ -158,8 +161,8 @@ __device__ __forceinline__ void rys_root_one(double T, int r, double &u, double 
     if (T < kRysTmax[NR]) {
         const int iv = (int)(T * (1.0 / PFK_RYS_H));
         const double x = (T - iv * PFK_RYS_H) * (2.0 / PFK_RYS_H) - 1.0;
-        const double *base = kRysCheb + kRysOffset[NR] + iv * (2 * NR) * (PFK_RYS_DEG + 1);
-        clenshaw_pair(base + r * 2 * (PFK_RYS_DEG + 1), x, u, w);
+        const int nint = kRysNint[NR];
+        clenshaw_pair(kRysCheb + kRysOffset[NR] + 2 * iv + 2 * r * nint, NR * nint, x, u, w);
     } else {
         const double iT = 1.0 / T;
         u = kRysAsymU[NR][r] * iT;

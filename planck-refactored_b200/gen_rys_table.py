@@ -23,9 +23,11 @@ Output: csrc/rys_table_data.inc (C initialisers, committed; regenerate with
 `python gen_rys_table.py`).  The includer defines PFK_RYS_CONST_STORAGE and
 PFK_RYS_TABLE_STORAGE (e.g. `static __constant__ const` and
 `static __device__ const`) so every translation unit gets statically
-initialised device copies.  Layout: per n, per interval, per root r, the
-DEG+1 Chebyshev coefficients of u_r and w_r interleaved (u_0, w_0, u_1, w_1,
-...), so the device reads one (u, w) coefficient pair per 16-byte load.  The script also prints the measured maximum
+initialised device copies.  Layout: per n, per coefficient degree k, per
+root r, the (u_r, w_r) coefficient pair of every interval in turn.  The
+device reads one (u, w) pair per 16-byte load, and the lanes of a warp,
+whose T fall in different intervals, read neighbouring pairs of the same
+(k, r) slab, which keeps each load within a few cache lines.  The script also prints the measured maximum
 interpolation error at random T against fresh 80-digit evaluations.
 """
 import multiprocessing as mproc
@@ -197,13 +199,15 @@ def main():
             off += layout[n - 1] * 2 * n * N
         f.write("PFK_RYS_CONST_STORAGE int kRysOffset[PFK_RYS_NMAX + 1] = {" + ", ".join(str(o) for o in offs) + "};\n")
         f.write(f"#define PFK_RYS_TABLE_SIZE {off}\n")
+        f.write("PFK_RYS_CONST_STORAGE int kRysNint[PFK_RYS_NMAX + 1] = {0, " +
+                ", ".join(str(layout[n - 1]) for n in range(1, NMAX + 1)) + "};\n")
         f.write("PFK_RYS_TABLE_STORAGE double __align__(16) kRysCheb[PFK_RYS_TABLE_SIZE] = {\n")
         for n in range(1, NMAX + 1):
-            f.write(f"// n = {n}: {layout[n-1]} intervals x {n} roots x {N} coefficients x (u, w)\n")
-            for i in range(layout[n - 1]):
+            f.write(f"// n = {n}: {N} coefficients x {n} roots x {layout[n-1]} intervals x (u, w)\n")
+            for k in range(N):
                 for r in range(n):
-                    f.write(",".join(f"{cu:.17g},{cw:.17g}" for cu, cw in
-                                     zip(tables[n][i][r], tables[n][i][n + r])) + ",\n")
+                    f.write(",".join(f"{tables[n][i][r][k]:.17g},{tables[n][i][n + r][k]:.17g}"
+                                     for i in range(layout[n - 1])) + ",\n")
         f.write("};\n")
         # large-T limit constants: x_i^2 and W_i for each n
         f.write("PFK_RYS_CONST_STORAGE double kRysAsymU[PFK_RYS_NMAX + 1][PFK_RYS_NMAX] = {{0},\n")

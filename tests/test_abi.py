@@ -154,10 +154,11 @@ def test_device_rys_table_reproduces_boys_moments():
             if T < tmax[n]:
                 iv = int(T / 2.0)
                 x = (T - iv * 2.0) - 1.0
-                base = off[n] + iv * 2 * n * 15
-                # per root: 15 (u_k, w_k) coefficient pairs
-                u = np.array([_cheb(cheb[base + r * 30: base + r * 30 + 30: 2], x) for r in range(n)])
-                w = np.array([_cheb(cheb[base + r * 30 + 1: base + r * 30 + 30: 2], x) for r in range(n)])
+                nint = int(round(tmax[n] / 2.0))
+                # layout [k][root][interval][u, w]
+                idx = lambda k, r: off[n] + 2 * ((k * n + r) * nint + iv)
+                u = np.array([_cheb([cheb[idx(k, r)] for k in range(15)], x) for r in range(n)])
+                w = np.array([_cheb([cheb[idx(k, r) + 1] for k in range(15)], x) for r in range(n)])
             else:
                 u = np.array(au[n - 1]) / T
                 w = np.array(aw[n - 1]) / np.sqrt(T)
