@@ -148,6 +148,31 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
  * roofline denominator of the integral kernels. */
 pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
+/* Size of the device scratch array behind pfk_fock_rhf_noalloc: 64 MiB,
+ * held by every GPU that loads the library until the process exits. */
+#define PFK_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* RHF build G = J(P) - K(P)/2 that allocates no device memory.  It has no
+ * counterpart in the reference.  It is for callers that must not call
+ * cudaMalloc or any allocator -- a host program whose GPU memory is owned by
+ * another allocator or pool, or one whose memory budget is fixed up front.
+ * Every device buffer the build needs (pair data, Schwarz table, screened
+ * quartet list, J and K accumulators) lives in one static device array of
+ * PFK_NOALLOC_SCRATCH_BYTES; a basis whose data does not fit is rejected with
+ * PFK_ERR_UNSUPPORTED and a message giving the bytes needed (roughly up to
+ * 200 basis functions of 6-31G** fit).
+ *   basis   host shell data, as for pfk_create
+ *   dP, dG  nbasis x nbasis densities / result on the current CUDA device
+ *   stream  cudaStream_t for the work (NULL: the default stream); the call
+ *           synchronises it and returns with dG written.
+ * The first call on a device looks up the scratch array's device address and
+ * sets kernel attributes on that device; make that first call before any
+ * stream capture.  All calls on a device share the one array: calls that
+ * overlap on the GPU (other host threads, other streams) race and must be
+ * serialised by the caller.  Each call clears what it needs at zero. */
+pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const double *dP, double *dG, double tol_eri,
+                                void *stream);
+
 #ifdef __cplusplus
 }
 #endif

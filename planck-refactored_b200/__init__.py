@@ -29,7 +29,8 @@ ENGINES = {"os": 0, "rys": 1, "auto": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
-           "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak"]
+           "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
+           "pfk_fock_rhf_noalloc"]
 
 _lib = None
 
@@ -74,6 +75,7 @@ def load_library(path=LIB_PATH):
     L.pfk_class_stats.argtypes = [vp, vp, vp, vp]
     L.pfk_set_shard.argtypes = [vp, c_int, c_int]
     L.pfk_measure_fma_peak.argtypes = [c_int, ctypes.POINTER(c_dbl), ctypes.POINTER(c_dbl)]
+    L.pfk_fock_rhf_noalloc.argtypes = [ctypes.POINTER(BasisDesc), vp, vp, c_dbl, vp]
     _lib = L
     return L
 

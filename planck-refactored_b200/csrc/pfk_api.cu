@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -822,3 +823,250 @@ pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tf
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free RHF build (pfk_fock_rhf_noalloc).
+//
+// For callers that may not allocate device memory -- code that runs inside a
+// host application whose GPU memory is owned by another allocator or pool,
+// or whose memory budget is fixed up front -- every device buffer this build
+// needs (shell-pair and primitive-pair data, the Schwarz table, the screened
+// quartet list, the J and K accumulators) is carved out of one file-scope
+// array of PFK_NOALLOC_SCRATCH_BYTES.  Every GPU that loads this library
+// holds that array until the process exits.
+// ===========================================================================
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PFK_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The name
+// g_noalloc_scratch in host code is only a host-side stand-in, so the
+// address is looked up once per device (with that device current) and
+// cached; the same first call also sets the class kernels' shared-memory
+// limits on that device.
+pfk_status noalloc_setup(int dev, unsigned char **out, std::string &why)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (dev < 0 || dev >= kNoallocMaxDevices) {
+        why = "device ordinal out of range for the allocation-free build";
+        return PFK_ERR_UNSUPPORTED;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            why = std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e);
+            return PFK_ERR_CUDA;
+        }
+        JKArgs none{};
+        for (int c = 0; c < kQuartetClasses; ++c) {
+            if (!g_class_launchers[c]) {
+                why = "class kernel table incomplete";
+                return PFK_ERR_STATE;
+            }
+            g_class_launchers[c](nullptr, -1, none, 1, nullptr);
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            why = std::string("kernel configuration: ") + cudaGetErrorString(e);
+            return PFK_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return PFK_OK;
+}
+
+// Bump allocation inside the scratch array (256-byte aligned pieces).
+struct ScratchCarver {
+    unsigned char *base;
+    size_t used = 0;
+    template <typename T>
+    T *take(size_t count)
+    {
+        const size_t off = (used + 255) & ~size_t(255);
+        used = off + sizeof(T) * count;
+        return reinterpret_cast<T *>(base + off);
+    }
+};
+
+template <typename T>
+size_t carve_size(size_t used, size_t count)
+{
+    return ((used + 255) & ~size_t(255)) + sizeof(T) * count;
+}
+
+}  // namespace
+
+extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const double *dP, double *dG, double tol_eri,
+                                           void *stream)
+{
+    std::string why;
+    pfk_status vs = validate(basis, why);
+    if (vs != PFK_OK) {
+        g_last_error = "pfk_fock_rhf_noalloc: " + why;
+        return vs;
+    }
+    if (!dP || !dG || !(tol_eri >= 0.0) || !std::isfinite(tol_eri)) {
+        g_last_error = "pfk_fock_rhf_noalloc: null matrix or bad tol_eri";
+        return PFK_ERR_INVALID;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("pfk_fock_rhf_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
+        return PFK_ERR_CUDA;
+    }
+    unsigned char *scratch = nullptr;
+    vs = noalloc_setup(dev, &scratch, why);
+    if (vs != PFK_OK) {
+        g_last_error = "pfk_fock_rhf_noalloc: " + why;
+        return vs;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    // host-side shell-pair data, as pfk_create builds it
+    pfk_ctx h;
+    h.nshell = basis->nshell;
+    h.bf_off.resize(basis->nshell);
+    int nb = 0;
+    for (int s = 0; s < basis->nshell; ++s) {
+        h.bf_off[s] = nb;
+        nb += ncart(basis->L[s]);
+    }
+    h.nb = nb;
+    build_pairs(&h, basis);
+    const size_t nb2 = (size_t)nb * nb;
+
+    // everything but the quartet list, checked before the device is touched
+    size_t need = 0;
+    need = carve_size<PairInfo>(need, h.npairs);
+    need = carve_size<PrimPair>(need, h.prims.size());
+    need = carve_size<int>(need, h.npairs);
+    need = carve_size<double>(need, nb2);
+    need = carve_size<double>(need, nb2);
+    need = carve_size<double>(need, nb2);
+    if (need > PFK_NOALLOC_SCRATCH_BYTES) {
+        g_last_error = "pfk_fock_rhf_noalloc: basis needs " + std::to_string(need) +
+                       " bytes of scratch before the quartet list; the limit is " +
+                       std::to_string((size_t)PFK_NOALLOC_SCRATCH_BYTES) + " bytes";
+        return PFK_ERR_UNSUPPORTED;
+    }
+    ScratchCarver cv{scratch};
+    PairInfo *d_pairs = cv.take<PairInfo>(h.npairs);
+    PrimPair *d_prims = cv.take<PrimPair>(h.prims.size());
+    int *d_ids = cv.take<int>(h.npairs);
+    double *d_Q = cv.take<double>(nb2);
+    double *d_J = cv.take<double>(nb2);
+    double *d_K = cv.take<double>(nb2);
+
+#define PFK_NA_CK(call)                                                                           \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            g_last_error = std::string("pfk_fock_rhf_noalloc: " #call ": ") + cudaGetErrorString(e_); \
+            return PFK_ERR_CUDA;                                                                 \
+        }                                                                                        \
+    } while (0)
+
+    // Schwarz table (the array keeps the previous call's contents: clear it)
+    std::vector<int> ids;
+    std::vector<int> cls_begin(kPairClasses + 1, 0);
+    for (int x = 0; x < kPairClasses; ++x) {
+        cls_begin[x] = (int)ids.size();
+        for (int p = 0; p < h.npairs; ++p)
+            if (h.pair_pc[p] == x) ids.push_back(p);
+    }
+    cls_begin[kPairClasses] = (int)ids.size();
+    PFK_NA_CK(cudaMemcpyAsync(d_pairs, h.pairs.data(), sizeof(PairInfo) * h.npairs, cudaMemcpyHostToDevice, st));
+    PFK_NA_CK(cudaMemcpyAsync(d_prims, h.prims.data(), sizeof(PrimPair) * h.prims.size(), cudaMemcpyHostToDevice, st));
+    PFK_NA_CK(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, st));
+    PFK_NA_CK(cudaMemsetAsync(d_Q, 0, sizeof(double) * nb2, st));
+    for (int x = 0; x < kPairClasses; ++x)
+        launch_schwarz(x, d_ids + cls_begin[x], cls_begin[x + 1] - cls_begin[x], d_pairs, d_prims, d_Q, nb, st);
+    PFK_NA_CK(cudaGetLastError());
+    std::vector<double> Q(nb2);
+    PFK_NA_CK(cudaMemcpyAsync(Q.data(), d_Q, sizeof(double) * nb2, cudaMemcpyDeviceToHost, st));
+    PFK_NA_CK(cudaStreamSynchronize(st));
+
+    // per-pair bounds, Q-sorted class lists, screened shell-quartet lists
+    std::vector<int> sorted[kPairClasses];
+    for (int p = 0; p < h.npairs; ++p) {
+        PairInfo &pi = h.pairs[p];
+        const int na = ncart(h.pair_la[p]), nbb = ncart(h.pair_lb[p]);
+        double qmax = 0.0, qmin = INFINITY;
+        for (int a = 0; a < na; ++a)
+            for (int c = 0; c < nbb; ++c) {
+                const double q = Q[(size_t)(pi.bf_a + a) * nb + pi.bf_b + c];
+                qmax = std::max(qmax, q);
+                qmin = std::min(qmin, q);
+            }
+        pi.qmax = qmax;
+        pi.qmin = qmin;
+        sorted[h.pair_pc[p]].push_back(p);
+    }
+    for (auto &v : sorted)
+        std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return h.pairs[a].qmax > h.pairs[b].qmax; });
+    std::vector<uint2> quart;
+    long long cls_off[kQuartetClasses + 1] = {};
+    for (int x = 0; x < kPairClasses; ++x)
+        for (int y = 0; y <= x; ++y) {
+            const int cls = quartet_class(x, y);
+            cls_off[cls] = (long long)quart.size();
+            const auto &X = sorted[x], &Y = sorted[y];
+            for (size_t a = 0; a < X.size(); ++a) {
+                const double qa = h.pairs[X[a]].qmax;
+                size_t lo = 0, hi = Y.size();   // kets kept: a prefix of the Q-sorted list
+                while (lo < hi) {
+                    const size_t mid = (lo + hi) / 2;
+                    if (qa * h.pairs[Y[mid]].qmax >= tol_eri) lo = mid + 1;
+                    else hi = mid;
+                }
+                for (size_t b = (x == y ? a : 0); b < lo; ++b)
+                    quart.push_back(make_uint2((unsigned)X[a], (unsigned)Y[b]));
+            }
+        }
+    // (x, y) visits the classes in increasing class index, so cls_off holds
+    // each class's start and the next class's start is its end
+    cls_off[kQuartetClasses] = (long long)quart.size();
+    const size_t total = carve_size<uint2>(cv.used, quart.size());
+    if (total > PFK_NOALLOC_SCRATCH_BYTES) {
+        g_last_error = "pfk_fock_rhf_noalloc: basis needs " + std::to_string(total) +
+                       " bytes of scratch with its screened quartet list; the limit is " +
+                       std::to_string((size_t)PFK_NOALLOC_SCRATCH_BYTES) + " bytes";
+        return PFK_ERR_UNSUPPORTED;
+    }
+    uint2 *d_q = cv.take<uint2>(quart.size());
+    PFK_NA_CK(cudaMemcpyAsync(d_pairs, h.pairs.data(), sizeof(PairInfo) * h.npairs, cudaMemcpyHostToDevice, st));
+    if (!quart.empty())
+        PFK_NA_CK(cudaMemcpyAsync(d_q, quart.data(), sizeof(uint2) * quart.size(), cudaMemcpyHostToDevice, st));
+
+    // the build: accumulators start at zero on every call
+    PFK_NA_CK(cudaMemsetAsync(d_J, 0, sizeof(double) * nb2, st));
+    PFK_NA_CK(cudaMemsetAsync(d_K, 0, sizeof(double) * nb2, st));
+    JKArgs a{};
+    a.pairs = d_pairs;
+    a.prims = d_prims;
+    a.Qao = d_Q;
+    a.Pj = dP;
+    a.Pk0 = dP;
+    a.Jacc = d_J;
+    a.Kacc0 = d_K;
+    a.tol = tol_eri;
+    a.nb = nb;
+    a.qstride = 1;
+    a.qoffset = 0;
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        const long long n = cls_off[c + 1] - cls_off[c];
+        if (n > 0) g_class_launchers[c](d_q + cls_off[c], n, a, 1, st);
+    }
+    PFK_NA_CK(cudaGetLastError());
+    PFK_NA_CK(combine(d_J, d_K, 1.0, -0.5, dG, nb, st));
+    PFK_NA_CK(cudaStreamSynchronize(st));
+#undef PFK_NA_CK
+    return PFK_OK;
+}
