@@ -421,8 +421,8 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         const long long nh = local(ctx->q_cnt[c]), nl = local(ctx->q32_cnt[c]);
         if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
-        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, st);
-        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, st);
+        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, 0, st);
+        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, ctx->precision == PFK_PREC_MIXED, st);
         PFK_CK(cudaGetLastError());
         if (timed) {
             PFK_CK(cudaEventRecord(ev[1], st));
@@ -540,7 +540,7 @@ pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
             ctx->launch[c] = g_class_launchers[c];
         }
         JKArgs none{};
-        for (int c = 0; c < kQuartetClasses; ++c) ctx->launch[c](nullptr, -1, none, 1, ctx->stream);
+        for (int c = 0; c < kQuartetClasses; ++c) ctx->launch[c](nullptr, -1, none, 1, 0, ctx->stream);
         e = cudaGetLastError();
         if (e != cudaSuccess) return bail(ctx->cuda_fail("kernel configuration", e));
         s = schwarz_and_sort(ctx);
@@ -868,7 +868,7 @@ pfk_status noalloc_setup(int dev, unsigned char **out, std::string &why)
                 why = "class kernel table incomplete";
                 return PFK_ERR_STATE;
             }
-            g_class_launchers[c](nullptr, -1, none, 1, nullptr);
+            g_class_launchers[c](nullptr, -1, none, 1, 0, nullptr);
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) {
@@ -1062,7 +1062,7 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
     a.qoffset = 0;
     for (int c = 0; c < kQuartetClasses; ++c) {
         const long long n = cls_off[c + 1] - cls_off[c];
-        if (n > 0) g_class_launchers[c](d_q + cls_off[c], n, a, 1, st);
+        if (n > 0) g_class_launchers[c](d_q + cls_off[c], n, a, 1, 0, st);
     }
     PFK_NA_CK(cudaGetLastError());
     PFK_NA_CK(combine(d_J, d_K, 1.0, -0.5, dG, nb, st));

@@ -14,7 +14,7 @@ namespace {
 constexpr int kRegMaxComponents = 81;   // register path up to (pp|pp)-sized blocks
 
 template <int LA, int LB, int LC, int LD>
-void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, cudaStream_t st)
+void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int fp32, cudaStream_t st)
 {
     using S = ClassShape<LA, LB, LC, LD>;
     using SS = SplitShape<LA, LB, LC, LD>;
@@ -23,6 +23,7 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, cudaStre
         if (n <= 0) return;
         const long long grid = (n + 127) / 128;
         if (nk == 2) eri_reg_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+        else if (fp32) eri_reg_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
         else eri_reg_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
     } else if constexpr (SS::OK) {
         if (n < 0) {  // configure the current device (shared-memory opt-in)

@@ -14,8 +14,11 @@ __host__ __device__ constexpr int pc_la(int pc) { return pc >= 6 ? 3 : pc >= 3 ?
 __host__ __device__ constexpr int pc_lb(int pc) { return pc - pc_la(pc) * (pc_la(pc) + 1) / 2; }
 __host__ __device__ constexpr int quartet_class(int bra_pc, int ket_pc) { return bra_pc * (bra_pc + 1) / 2 + ket_pc; }
 
-// One launcher per quartet class.  nk = number of exchange densities (1 or 2).
-using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, cudaStream_t st);
+// One launcher per quartet class.  nk = number of exchange densities (1 or 2);
+// fp32 != 0 asks for the FP32-arithmetic variant where the class has one
+// (register-path classes with nk == 1; the others run FP64).
+using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, int fp32,
+                               cudaStream_t st);
 
 // Launchers of the 55 classes, filled at library load by the pfk_classes.cu
 // units (each compiled for a range of classes).  A launcher called with

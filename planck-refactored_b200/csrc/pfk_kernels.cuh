@@ -69,7 +69,12 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
 // ---------------------------------------------------------------------------
 // Register path
 // ---------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD, int NK>
+// R is the arithmetic type of the 2D integrals, the transfer relations, the
+// product and the contraction: double, or float for the mixed-precision list
+// of quartets whose Schwarz bound is below the FP32 threshold.  Roots,
+// weights and the per-primitive-quartet scalars stay FP64 in both, and so
+// does the J/K digestion and accumulation.
+template <int LA, int LB, int LC, int LD, int NK, typename R = double>
 __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
 {
     using S = ClassShape<LA, LB, LC, LD>;
@@ -80,9 +85,9 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
 
-    double acc[NA * NB * NC * ND];
+    R acc[NA * NB * NC * ND];
 #pragma unroll
-    for (int c = 0; c < S::N; ++c) acc[c] = 0.0;
+    for (int c = 0; c < S::N; ++c) acc[c] = R(0);
 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
@@ -100,13 +105,13 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
                 const double B00 = 0.5 * s.rdelta * ur;
                 const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
                 const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
-                double gx[NI], gy[NI], gz[NI];
-                axis_table<LA, LB, LC, LD, double>(p.PAx + ur * s.WPx, q.PAx + ur * s.WQx, B00, B10, B01,
-                                                   pb.ABx, pk.ABx, w[r] * s.pref, gx);
-                axis_table<LA, LB, LC, LD, double>(p.PAy + ur * s.WPy, q.PAy + ur * s.WQy, B00, B10, B01,
-                                                   pb.ABy, pk.ABy, 1.0, gy);
-                axis_table<LA, LB, LC, LD, double>(p.PAz + ur * s.WPz, q.PAz + ur * s.WQz, B00, B10, B01,
-                                                   pb.ABz, pk.ABz, 1.0, gz);
+                R gx[NI], gy[NI], gz[NI];
+                axis_table<LA, LB, LC, LD, R>(R(p.PAx + ur * s.WPx), R(q.PAx + ur * s.WQx), R(B00), R(B10),
+                                              R(B01), R(pb.ABx), R(pk.ABx), R(w[r] * s.pref), gx);
+                axis_table<LA, LB, LC, LD, R>(R(p.PAy + ur * s.WPy), R(q.PAy + ur * s.WQy), R(B00), R(B10),
+                                              R(B01), R(pb.ABy), R(pk.ABy), R(1), gy);
+                axis_table<LA, LB, LC, LD, R>(R(p.PAz + ur * s.WPz), R(q.PAz + ur * s.WQz), R(B00), R(B10),
+                                              R(B01), R(pb.ABz), R(pk.ABz), R(1), gz);
 #pragma unroll
                 for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
@@ -143,7 +148,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
                                                          args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
                         if (sw != 0.0)
                             scatter8(args.eri_out, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id,
-                                     acc[c] * S::norm(ia, ib, ic, id));
+                                     double(acc[c]) * S::norm(ia, ib, ic, id));
                     }
         return;
     }
@@ -212,7 +217,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
                     const int c = ((ia * NB + ib) * NC + ic) * ND + id;
                     const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
                                                      args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
-                    const double v = acc[c] * (sw * S::norm(ia, ib, ic, id));
+                    const double v = double(acc[c]) * (sw * S::norm(ia, ib, ic, id));
                     jab[ia * NB + ib] += v * pcd[ic * ND + id];
                     jcd[ic * ND + id] += v * pab[ia * NB + ib];
 #pragma unroll
