@@ -354,6 +354,7 @@ def ours_arm(args):
                 "fp32_fma_peak_tflops": fp32_peak,
                 "classes_ms": {k: round(v[2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "classes_primitive_quartets": {k: v[1] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
+                "classes_shell_quartets": {k: v[0] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "clocks": clk}
         if mixed:
             line["mixed_precision"] = mixed

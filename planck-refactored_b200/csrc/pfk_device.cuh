@@ -36,7 +36,14 @@ __host__ __device__ constexpr int cart_lz(int L, int i)
     return i - cart_block(i) * (cart_block(i) + 1) / 2;
 }
 __host__ __device__ constexpr int cart_ly(int L, int i) { return L - cart_lx(L, i) - cart_lz(L, i); }
-__host__ __device__ constexpr int dfact(int n) { return n <= 0 ? 1 : n * dfact(n - 2); }
+// Iterative (not recursive) so that calls with unrolled-loop indices inline
+// and fold to constants instead of becoming device-side calls.
+__host__ __device__ constexpr int dfact(int n)
+{
+    int r = 1;
+    for (int k = n; k > 1; k -= 2) r *= k;
+    return r;
+}
 // 1/sqrt((2lx-1)!!(2ly-1)!!(2lz-1)!!) (src/basis/gaussian.cpp:283-296); the
 // double factorials for L <= 3 are 1, 1, 3, 15, so the square roots below are
 // of small integers.

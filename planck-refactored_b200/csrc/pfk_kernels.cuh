@@ -7,6 +7,9 @@
 //   eri_reg_kernel   one thread per shell quartet; the contracted Cartesian
 //                    block, the per-root axis tables and the J/K partial
 //                    sums all live in registers.  Used for small classes.
+//   eri_split_kernel a team of lanes per shell quartet sharing per-root
+//                    tables in shared memory; each lane owns A-component
+//                    slices of the block.  Larger classes.
 //   eri_team_kernel  a team of TEAM threads (a warp or the whole block) per
 //                    shell quartet; the per-root axis tables are built once
 //                    per primitive quartet into shared memory and every
@@ -64,6 +67,141 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
     }
     if (check && __ldg(Qao + (size_t)i * nb + j) * __ldg(Qao + (size_t)k * nb + l) < tol) return 0.0;
     return s;
+}
+
+
+// J/K digestion of one weighted Cartesian block v (index ((ia*NB+ib)*NC+ic)*ND+id),
+// one output block at a time so that only that block's density values and
+// partial sums are live next to v:
+//   J(i,j) += sum_kl v P(k,l)     J(k,l) += sum_ij v P(i,j)
+//   K(i,k) += sum_jl v Pk(j,l)    K(j,k) += sum_il v Pk(i,l)
+//   K(i,l) += sum_jk v Pk(j,k)    K(j,l) += sum_ik v Pk(i,k)
+// (J = 2 (Jacc + Jacc^T) and K = Kacc + Kacc^T afterwards.)
+template <int NA, int NB, int NC, int ND, int NK, typename V>
+__device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args)
+{
+    const int nb = args.nb;
+#define PFK_V(ia, ib, ic, id) double(v[(((ia) * NB + (ib)) * NC + (ic)) * ND + (id)])
+    {
+        double p[NC * ND];
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) p[ic * ND + id] = __ldg(args.Pj + (size_t)(k0 + ic) * nb + l0 + id);
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) {
+                double s = 0.0;
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ic * ND + id];
+                atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+            }
+    }
+    asm volatile("" ::: "memory");
+    {
+        double p[NA * NB];
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) p[ia * NB + ib] = __ldg(args.Pj + (size_t)(i0 + ia) * nb + j0 + ib);
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) {
+                double s = 0.0;
+#pragma unroll
+                for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                    for (int ib = 0; ib < NB; ++ib) s += PFK_V(ia, ib, ic, id) * p[ia * NB + ib];
+                atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, s);
+            }
+    }
+#pragma unroll
+    for (int m = 0; m < NK; ++m) {
+        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+        const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
+        if (!Kacc) continue;
+        asm volatile("" ::: "memory");
+        {   // K(i,k) from Pk(j,l)
+            double p[NB * ND];
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) p[ib * ND + id] = __ldg(Pk + (size_t)(j0 + ib) * nb + l0 + id);
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                        for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ib * ND + id];
+                    atomicAdd(Kacc + (size_t)(i0 + ia) * nb + k0 + ic, s);
+                }
+        }
+        asm volatile("" ::: "memory");
+        {   // K(j,k) from Pk(i,l)
+            double p[NA * ND];
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) p[ia * ND + id] = __ldg(Pk + (size_t)(i0 + ia) * nb + l0 + id);
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                        for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ia * ND + id];
+                    atomicAdd(Kacc + (size_t)(j0 + ib) * nb + k0 + ic, s);
+                }
+        }
+        asm volatile("" ::: "memory");
+        {   // K(i,l) from Pk(j,k)
+            double p[NB * NC];
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic) p[ib * NC + ic] = __ldg(Pk + (size_t)(j0 + ib) * nb + k0 + ic);
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                        for (int ic = 0; ic < NC; ++ic) s += PFK_V(ia, ib, ic, id) * p[ib * NC + ic];
+                    atomicAdd(Kacc + (size_t)(i0 + ia) * nb + l0 + id, s);
+                }
+        }
+        asm volatile("" ::: "memory");
+        {   // K(j,l) from Pk(i,k)
+            double p[NA * NC];
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic) p[ia * NC + ic] = __ldg(Pk + (size_t)(i0 + ia) * nb + k0 + ic);
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+                        for (int ic = 0; ic < NC; ++ic) s += PFK_V(ia, ib, ic, id) * p[ia * NC + ic];
+                    atomicAdd(Kacc + (size_t)(j0 + ib) * nb + l0 + id, s);
+                }
+        }
+    }
+#undef PFK_V
 }
 
 // ---------------------------------------------------------------------------
@@ -153,59 +291,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
         return;
     }
 
-    const double *__restrict__ Pj = args.Pj;
-    double jab[NA * NB], jcd[NC * ND];
-    double pab[NA * NB], pcd[NC * ND];
-#pragma unroll
-    for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib) {
-            jab[ia * NB + ib] = 0.0;
-            pab[ia * NB + ib] = __ldg(Pj + (size_t)(i0 + ia) * nb + j0 + ib);
-        }
-#pragma unroll
-    for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-        for (int id = 0; id < ND; ++id) {
-            jcd[ic * ND + id] = 0.0;
-            pcd[ic * ND + id] = __ldg(Pj + (size_t)(k0 + ic) * nb + l0 + id);
-        }
-    // exchange: four blocks per K density
-    double kac[NK][NA * NC], kbc[NK][NB * NC], kad[NK][NA * ND], kbd[NK][NB * ND];
-    double pac[NK][NA * NC], pbc[NK][NB * NC], pad_[NK][NA * ND], pbd[NK][NB * ND];
-#pragma unroll
-    for (int m = 0; m < NK; ++m) {
-        const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) {
-                kac[m][ia * NC + ic] = 0.0;
-                pac[m][ia * NC + ic] = __ldg(Pk + (size_t)(i0 + ia) * nb + k0 + ic);
-            }
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) {
-                kbc[m][ib * NC + ic] = 0.0;
-                pbc[m][ib * NC + ic] = __ldg(Pk + (size_t)(j0 + ib) * nb + k0 + ic);
-            }
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int id = 0; id < ND; ++id) {
-                kad[m][ia * ND + id] = 0.0;
-                pad_[m][ia * ND + id] = __ldg(Pk + (size_t)(i0 + ia) * nb + l0 + id);
-            }
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-            for (int id = 0; id < ND; ++id) {
-                kbd[m][ib * ND + id] = 0.0;
-                pbd[m][ib * ND + id] = __ldg(Pk + (size_t)(j0 + ib) * nb + l0 + id);
-            }
-    }
-
+    // weights (duplicates, AO-level screening) and component norms, in place
 #pragma unroll
     for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
@@ -217,47 +303,9 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
                     const int c = ((ia * NB + ib) * NC + ic) * ND + id;
                     const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
                                                      args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
-                    const double v = double(acc[c]) * (sw * S::norm(ia, ib, ic, id));
-                    jab[ia * NB + ib] += v * pcd[ic * ND + id];
-                    jcd[ic * ND + id] += v * pab[ia * NB + ib];
-#pragma unroll
-                    for (int m = 0; m < NK; ++m) {
-                        kac[m][ia * NC + ic] += v * pbd[m][ib * ND + id];
-                        kbc[m][ib * NC + ic] += v * pad_[m][ia * ND + id];
-                        kad[m][ia * ND + id] += v * pbc[m][ib * NC + ic];
-                        kbd[m][ib * ND + id] += v * pac[m][ia * NC + ic];
-                    }
+                    acc[c] = acc[c] * R(sw * S::norm(ia, ib, ic, id));
                 }
-
-#pragma unroll
-    for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib) atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, jab[ia * NB + ib]);
-#pragma unroll
-    for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-        for (int id = 0; id < ND; ++id) atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, jcd[ic * ND + id]);
-#pragma unroll
-    for (int m = 0; m < NK; ++m) {
-        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
-        if (!Kacc) continue;
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(i0 + ia) * nb + k0 + ic, kac[m][ia * NC + ic]);
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(j0 + ib) * nb + k0 + ic, kbc[m][ib * NC + ic]);
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(i0 + ia) * nb + l0 + id, kad[m][ia * ND + id]);
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(j0 + ib) * nb + l0 + id, kbd[m][ib * ND + id]);
-    }
+    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args);
 }
 
 // ---------------------------------------------------------------------------
@@ -616,51 +664,6 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
         return;
     }
 
-    const double *__restrict__ Pj = args.Pj;
-    double pcd[NC * ND], jcd[NC * ND];
-#pragma unroll
-    for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-        for (int id = 0; id < ND; ++id) {
-            pcd[ic * ND + id] = __ldg(Pj + (size_t)(k0 + ic) * nb + l0 + id);
-            jcd[ic * ND + id] = 0.0;
-        }
-    double jab[NBT], pab[NBT];
-#pragma unroll
-    for (int bl = 0; bl < NBT; ++bl) {
-        jab[bl] = 0.0;
-        pab[bl] = __ldg(Pj + (size_t)i * nb + j0 + ib0 + bl);
-    }
-    // exchange blocks: K(i,k) [NC], K(j,k) [NBT*NC], K(i,l) [ND], K(j,l) [NBT*ND]
-    double kac[NK][NC], kbc[NK][NBT * NC], kad[NK][ND], kbd[NK][NBT * ND];
-    double pac[NK][NC], pbc[NK][NBT * NC], pad_[NK][ND], pbd[NK][NBT * ND];
-#pragma unroll
-    for (int m = 0; m < NK; ++m) {
-        const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
-#pragma unroll
-        for (int ic = 0; ic < NC; ++ic) {
-            kac[m][ic] = 0.0;
-            pac[m][ic] = __ldg(Pk + (size_t)i * nb + k0 + ic);
-        }
-#pragma unroll
-        for (int id = 0; id < ND; ++id) {
-            kad[m][id] = 0.0;
-            pad_[m][id] = __ldg(Pk + (size_t)i * nb + l0 + id);
-        }
-#pragma unroll
-        for (int bl = 0; bl < NBT; ++bl) {
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) {
-                kbc[m][bl * NC + ic] = 0.0;
-                pbc[m][bl * NC + ic] = __ldg(Pk + (size_t)(j0 + ib0 + bl) * nb + k0 + ic);
-            }
-#pragma unroll
-            for (int id = 0; id < ND; ++id) {
-                kbd[m][bl * ND + id] = 0.0;
-                pbd[m][bl * ND + id] = __ldg(Pk + (size_t)(j0 + ib0 + bl) * nb + l0 + id);
-            }
-        }
-    }
 #pragma unroll
     for (int bl = 0; bl < NBT; ++bl)
 #pragma unroll
@@ -670,40 +673,11 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
                 const int ib = ib0 + bl;
                 const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao, nb,
                                                  i, j0 + ib, k0 + ic, l0 + id, args.tol);
-                const double nrm = cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
-                const double v = acc[(bl * NC + ic) * ND + id] * (sw * nrm);
-                jab[bl] += v * pcd[ic * ND + id];
-                jcd[ic * ND + id] += v * pab[bl];
-#pragma unroll
-                for (int m = 0; m < NK; ++m) {
-                    kac[m][ic] += v * pbd[m][bl * ND + id];
-                    kbc[m][bl * NC + ic] += v * pad_[m][id];
-                    kad[m][id] += v * pbc[m][bl * NC + ic];
-                    kbd[m][bl * ND + id] += v * pac[m][ic];
-                }
+                acc[(bl * NC + ic) * ND + id] *=
+                    sw * cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
             }
-#pragma unroll
-    for (int bl = 0; bl < NBT; ++bl) atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, jab[bl]);
-#pragma unroll
-    for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-        for (int id = 0; id < ND; ++id) atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, jcd[ic * ND + id]);
-#pragma unroll
-    for (int m = 0; m < NK; ++m) {
-        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
-        if (!Kacc) continue;
-#pragma unroll
-        for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)i * nb + k0 + ic, kac[m][ic]);
-#pragma unroll
-        for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)i * nb + l0 + id, kad[m][id]);
-#pragma unroll
-        for (int bl = 0; bl < NBT; ++bl) {
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic) atomicAdd(Kacc + (size_t)(j0 + ib0 + bl) * nb + k0 + ic, kbc[m][bl * NC + ic]);
-#pragma unroll
-            for (int id = 0; id < ND; ++id) atomicAdd(Kacc + (size_t)(j0 + ib0 + bl) * nb + l0 + id, kbd[m][bl * ND + id]);
-        }
-    }
+    digest_blocks<1, NBT, NC, ND, NK>(acc, i, j0 + ib0, k0, l0, args);
 }
 
 }  // namespace pfk
+
