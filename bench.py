@@ -205,7 +205,7 @@ def ours_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     atoms, mol, shells = build_shells(args.waters)
     t0 = time.perf_counter()
-    eng = P.FockEngine(shells, device=local, precision=args.precision, fp32_bound=1e-8)
+    eng = P.FockEngine(shells, device=local, engine=args.engine, precision=args.precision, fp32_bound=1e-8)
     t_setup = time.perf_counter() - t0
     if world > 1:
         eng.set_shard(rank, world)
@@ -302,7 +302,7 @@ def ours_arm(args):
         step()
         torch.cuda.synchronize()
         G_mixed = dG.cpu().numpy().copy()
-        e64 = P.FockEngine(shells, device=local, precision="fp64")
+        e64 = P.FockEngine(shells, device=local, engine=args.engine, precision="fp64")
         if world > 1:
             e64.set_shard(rank, world)
         ms64 = device_ms(e64, max(3, args.steps // 2))
@@ -317,6 +317,14 @@ def ours_arm(args):
     dP_host = Pm  # class_stats times a build on the context's current density
     eng.fock_rhf(dP_host)
     cls = eng.class_stats(timed=True)
+    cls_rys = None
+    if args.engine != "rys":   # the same classes on the Rys kernels, for the engine choice
+        er = P.FockEngine(shells, device=local, engine="rys", precision=args.precision, fp32_bound=1e-8)
+        if world > 1:
+            er.set_shard(rank, world)
+        er.fock_rhf(dP_host)
+        cls_rys = er.class_stats(timed=True)
+        er.close()
     fp64_peak, fp32_peak = P.measure_fma_peak(local)
     top = max(cls.items(), key=lambda kv: kv[1][2])
     top_flops = P.class_flops(top[0], top[1][1]) / world
@@ -332,7 +340,7 @@ def ours_arm(args):
                 "dtype": "f64" if args.precision == "fp64" else "f64+f32",
                 "data": "synthetic (seeded water cluster, Basis Set Exchange 6-31G**)",
                 "config": {"workload": WORKLOAD if args.waters == 32 else f"(H2O){args.waters} 6-31G** ({nb} bf)",
-                           "nbasis": nb, "tol_eri": 1e-10, "precision": args.precision,
+                           "nbasis": nb, "tol_eri": 1e-10, "precision": args.precision, "engine": args.engine,
                            "parallelism": f"quartet-list shards x{world} + NCCL all-reduce of G" if world > 1
                            else "single GPU", "l2": "inputs larger than L2: the screened quartet lists "
                            f"({n_shell * 8 / 1e9:.2f} GB) and primitive-pair data stream from HBM every build",
@@ -355,6 +363,8 @@ def ours_arm(args):
                 "classes_ms": {k: round(v[2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "classes_primitive_quartets": {k: v[1] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "classes_shell_quartets": {k: v[0] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
+                "classes_ms_rys_kernels": None if cls_rys is None else
+                {k: round(cls_rys[k][2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "clocks": clk}
         if mixed:
             line["mixed_precision"] = mixed
@@ -376,6 +386,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--engine", choices=["os", "rys", "auto"], default="os",
+                    help="integral engine (the reference's option; os is its default)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="mixed: FP32 below a Schwarz bound of 1e-8 (the benchmark configuration); "
                          "the all-FP64 build is timed beside it")

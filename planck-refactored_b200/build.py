@@ -26,7 +26,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC,
 
 DEVICE_DEPS = ["pfk_device.cuh", "pfk_internal.h", "rys_table_data.inc"]
 DEPS = {
-    "pfk_classes.cu": DEVICE_DEPS + ["pfk_kernels.cuh"],
+    "pfk_classes.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_os.cuh"],
     "pfk_setup.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_setup.h"],
     "pfk_api.cu": DEVICE_DEPS + ["pfk_setup.h", "../../include/planck_fock.h"],
 }

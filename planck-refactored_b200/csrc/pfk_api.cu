@@ -218,6 +218,16 @@ pfk_status upload_pairs(pfk_ctx *ctx)
 }
 
 // Screened shell-quartet lists for the current tol / FP32 bound.
+// Releases the captured RHF builds; the next device call captures again.
+void drop_graphs(pfk_ctx *ctx)
+{
+    for (auto &g : ctx->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->graphs.clear();
+}
+
 pfk_status build_lists(pfk_ctx *ctx)
 {
     const double bound = ctx->precision == PFK_PREC_MIXED ? ctx->fp32_bound : 0.0;
@@ -316,11 +326,7 @@ pfk_status build_lists(pfk_ctx *ctx)
         PFK_CK(cudaStreamSynchronize(ctx->stream));
     }
     PFK_CK(cudaStreamSynchronize(ctx->stream));
-    for (auto &g : ctx->graphs) {   // captured builds refer to the old lists
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-        if (g.graph) cudaGraphDestroy(g.graph);
-    }
-    ctx->graphs.clear();
+    drop_graphs(ctx);   // captured builds refer to the old lists
     return PFK_OK;
 }
 
@@ -421,8 +427,13 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         const long long nh = local(ctx->q_cnt[c]), nl = local(ctx->q32_cnt[c]);
         if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
-        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, 0, st);
-        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, ctx->precision == PFK_PREC_MIXED, st);
+        // engine os / auto: Obara-Saika kernels for the classes that have them
+        // (L <= kOSMaxL, where the reference's per-quartet auto choice is OS
+        // for every component quartet), Rys for the rest; engine rys: Rys.
+        const int os = (ctx->engine != PFK_ENGINE_RYS && quartet_class_L(c) <= kOSMaxL) ? kLaunchOS : 0;
+        const int fp32 = ctx->precision == PFK_PREC_MIXED ? kLaunchFP32 : 0;
+        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, os, st);
+        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, os | fp32, st);
         PFK_CK(cudaGetLastError());
         if (timed) {
             PFK_CK(cudaEventRecord(ev[1], st));
@@ -599,6 +610,7 @@ pfk_status pfk_set_options(pfk_ctx *ctx, double tol_eri, int engine, int precisi
     cudaSetDevice(ctx->device);
     const bool rebuild = tol_eri != ctx->tol || precision != ctx->precision ||
                          (precision == PFK_PREC_MIXED && fp32_bound != ctx->fp32_bound);
+    if (engine != ctx->engine) drop_graphs(ctx);   // captured builds hold the old engine's kernels
     ctx->tol = tol_eri;
     ctx->engine = engine;
     ctx->precision = precision;
@@ -804,11 +816,7 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
     if (nranks < 1 || rank < 0 || rank >= nranks) return ctx->fail(PFK_ERR_INVALID, "need 0 <= rank < nranks");
     ctx->shard_rank = rank;
     ctx->shard_n = nranks;
-    for (auto &g : ctx->graphs) {
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-        if (g.graph) cudaGraphDestroy(g.graph);
-    }
-    ctx->graphs.clear();
+    drop_graphs(ctx);
     return PFK_OK;
 }
 

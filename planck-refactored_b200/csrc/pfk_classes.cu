@@ -3,6 +3,7 @@
 // 55 class instantiations build in parallel).
 #include "pfk_internal.h"
 #include "pfk_kernels.cuh"
+#include "pfk_os.cuh"
 
 #if !defined(PFK_CLASS_BEGIN) || !defined(PFK_CLASS_END)
 #error "PFK_CLASS_BEGIN and PFK_CLASS_END must be defined (0 <= begin < end <= 55)"
@@ -14,11 +15,22 @@ namespace {
 constexpr int kRegMaxComponents = 81;   // register path up to (pp|pp)-sized blocks
 
 template <int LA, int LB, int LC, int LD>
-void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int fp32, cudaStream_t st)
+void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int flags, cudaStream_t st)
 {
     using S = ClassShape<LA, LB, LC, LD>;
     using SS = SplitShape<LA, LB, LC, LD>;
     using TS = TeamShape<LA, LB, LC, LD>;
+    const int fp32 = flags & kLaunchFP32;
+    if constexpr (LA + LB + LC + LD <= kOSMaxL) {
+        if (flags & kLaunchOS) {
+            if (n <= 0) return;
+            const long long grid = (n + 127) / 128;
+            if (nk == 2) eri_os_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else if (fp32) eri_os_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else eri_os_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            return;
+        }
+    }
     if constexpr (S::N <= kRegMaxComponents) {
         if (n <= 0) return;
         const long long grid = (n + 127) / 128;

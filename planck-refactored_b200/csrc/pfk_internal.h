@@ -13,11 +13,24 @@ __host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la +
 __host__ __device__ constexpr int pc_la(int pc) { return pc >= 6 ? 3 : pc >= 3 ? 2 : pc >= 1 ? 1 : 0; }
 __host__ __device__ constexpr int pc_lb(int pc) { return pc - pc_la(pc) * (pc_la(pc) + 1) / 2; }
 __host__ __device__ constexpr int quartet_class(int bra_pc, int ket_pc) { return bra_pc * (bra_pc + 1) / 2 + ket_pc; }
+// Total angular momentum LA+LB+LC+LD of quartet class c.
+__host__ __device__ constexpr int quartet_class_L(int c)
+{
+    int x = 0;
+    while ((x + 1) * (x + 2) / 2 <= c) ++x;
+    const int y = c - x * (x + 1) / 2;
+    return pc_la(x) + pc_lb(x) + pc_la(y) + pc_lb(y);
+}
 
-// One launcher per quartet class.  nk = number of exchange densities (1 or 2);
-// fp32 != 0 asks for the FP32-arithmetic variant where the class has one
-// (register-path classes with nk == 1; the others run FP64).
-using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, int fp32,
+// Launch flags.  kLaunchFP32 asks for the FP32-arithmetic variant where the
+// class has one (register-path and Obara-Saika classes with nk == 1; the
+// others run FP64).  kLaunchOS asks for the Obara-Saika kernel, which exists
+// for classes with LA+LB+LC+LD <= kOSMaxL; the other classes run Rys.
+constexpr int kLaunchFP32 = 1, kLaunchOS = 2;
+constexpr int kOSMaxL = 4;
+
+// One launcher per quartet class.  nk = number of exchange densities (1 or 2).
+using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs &args, int nk, int flags,
                                cudaStream_t st);
 
 // Launchers of the 55 classes, filled at library load by the pfk_classes.cu

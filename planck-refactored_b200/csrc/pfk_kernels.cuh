@@ -204,6 +204,56 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
 #undef PFK_V
 }
 
+// Weights (duplicate components, AO-level screening), component norms and
+// J/K digestion of a contracted Cartesian block acc[((ia*NB+ib)*NC+ic)*ND+id]
+// of one shell quartet; in dense-tensor mode the block is scattered instead.
+template <int LA, int LB, int LC, int LD, int NK, typename R>
+__device__ __forceinline__ void finish_block(R *acc, const uint2 qd, const PairInfo &pb, const PairInfo &pk,
+                                             const JKArgs &args)
+{
+    using S = ClassShape<LA, LB, LC, LD>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
+    const int nb = args.nb;
+    const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
+    const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
+    const bool check = pb.qmin * pk.qmin < args.tol;
+
+    if (args.eri_out) {
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) {
+                        const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                        const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
+                                                         args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
+                        if (sw != 0.0)
+                            scatter8(args.eri_out, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id,
+                                     double(acc[c]) * S::norm(ia, ib, ic, id));
+                    }
+        return;
+    }
+
+    // weights (duplicates, AO-level screening) and component norms, in place
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                    const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
+                                                     args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
+                    acc[c] = acc[c] * R(sw * S::norm(ia, ib, ic, id));
+                }
+    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args);
+}
+
 // ---------------------------------------------------------------------------
 // Register path
 // ---------------------------------------------------------------------------
@@ -266,46 +316,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
         }
     }
 
-    // ---- digestion ----
-    const int nb = args.nb;
-    const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
-    const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
-    const bool check = pb.qmin * pk.qmin < args.tol;
-
-    if (args.eri_out) {
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-                for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-                    for (int id = 0; id < ND; ++id) {
-                        const int c = ((ia * NB + ib) * NC + ic) * ND + id;
-                        const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
-                                                         args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
-                        if (sw != 0.0)
-                            scatter8(args.eri_out, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id,
-                                     double(acc[c]) * S::norm(ia, ib, ic, id));
-                    }
-        return;
-    }
-
-    // weights (duplicates, AO-level screening) and component norms, in place
-#pragma unroll
-    for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-        for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-            for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-                for (int id = 0; id < ND; ++id) {
-                    const int c = ((ia * NB + ib) * NC + ic) * ND + id;
-                    const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check,
-                                                     args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
-                    acc[c] = acc[c] * R(sw * S::norm(ia, ib, ic, id));
-                }
-    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args);
+    finish_block<LA, LB, LC, LD, NK, R>(acc, qd, pb, pk, args);
 }
 
 // ---------------------------------------------------------------------------

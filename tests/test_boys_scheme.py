@@ -1,0 +1,66 @@
+"""The Boys-function scheme of the Obara-Saika kernels (CPU test).
+
+boys_fm<M> in csrc/pfk_os.cuh evaluates F_0..F_M (M <= 4) as follows:
+  * T below TS (1 for M <= 1, 2 otherwise): the Taylor series of F_M,
+    sum_k (-T)^k / (k! (2M+2k+1)), with 18 (M <= 1) or 25 terms, then the
+    downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1);
+  * otherwise F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward recursion
+    F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
+This test restates that scheme in double precision with the C library's erf
+and exp and checks it against 40-digit Boys values.  The scheme's parameters
+(thresholds, term counts) are what the device code uses.  The device's erf
+and exp differ from the C library's by a few ulp, which the GPU integral tests
+cover."""
+import math
+
+import numpy as np
+import pytest
+
+mpmath = pytest.importorskip("mpmath")
+
+
+def _coef(M, k):
+    return (-1) ** k / (math.factorial(k) * (2 * M + 2 * k + 1))
+
+
+def boys_scheme(M, T):
+    TS, NT = (1.0, 18) if M <= 1 else (2.0, 25)
+    F = [0.0] * (M + 1)
+    if T < TS:
+        s = _coef(M, NT - 1)
+        for k in range(NT - 2, -1, -1):
+            s = s * T + _coef(M, k)
+        F[M] = s
+        e = math.exp(-T)
+        for m in range(M - 1, -1, -1):
+            F[m] = (2.0 * T * F[m + 1] + e) * (1.0 / (2 * m + 1))
+    else:
+        ist = 1.0 / math.sqrt(T)
+        F[0] = 0.88622692545275801365 * math.erf(T * ist) * ist
+        e = math.exp(-T)
+        h = 0.5 * ist * ist
+        for m in range(M):
+            F[m + 1] = ((2 * m + 1) * F[m] - e) * h
+    return F
+
+
+def boys_exact(m, T):
+    with mpmath.workdps(40):
+        T = mpmath.mpf(T)
+        if T == 0:
+            return mpmath.mpf(1) / (2 * m + 1)
+        return mpmath.gammainc(m + mpmath.mpf(1) / 2, 0, T) / (2 * T ** (m + mpmath.mpf(1) / 2))
+
+
+@pytest.mark.parametrize("M,bound", [(0, 1e-15), (1, 2e-15), (2, 4e-15), (3, 8e-15), (4, 2e-14)])
+def test_boys_scheme_relative_error(M, bound):
+    rng = np.random.default_rng(M)
+    Ts = np.concatenate([rng.uniform(0, 3, 150), rng.uniform(0, 80, 150), np.logspace(-14, 3, 40),
+                         [0.0, 0.999999999, 1.0, 1.000000001, 1.999999999, 2.0, 2.000000001]])
+    worst = 0.0
+    for T in Ts:
+        F = boys_scheme(M, float(T))
+        for m in range(M + 1):
+            ref = boys_exact(m, T)
+            worst = max(worst, float(abs((F[m] - ref) / ref)))
+    assert worst < bound, worst

@@ -1,0 +1,98 @@
+"""The two device integral engines (GPU tests).
+
+`engine os` and `engine auto` run the Obara-Saika kernels (pfk_os.cuh) for
+every class with LA+LB+LC+LD <= 4 -- the classes where the reference's
+per-quartet auto choice picks OS for every component quartet (rys.cpp:195-236)
+-- and the Rys kernels for the larger classes; `engine rys` runs Rys for all
+classes.  The two engines evaluate the same integrals by different
+recurrences, so they must agree to rounding, and each must match the oracle's
+restatement of the corresponding reference engine."""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import WATER, basis_library, pfk, random_density, random_shells
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def random_basis():
+    # s, p and d shells, contraction depth 1-6, exponents up to 1e4, centres
+    # in a 2.5 Angstrom cube: every class up to (dd|dd) is present
+    return random_shells(9, lmax=2, seed=21, box=2.5)
+
+
+def test_os_and_rys_kernels_agree(random_basis):
+    P = pfk()
+    eng = P.FockEngine(random_basis, engine="os")
+    eri_os = eng.eri_tensor()
+    eng.set_options(1e-10, "rys")
+    eri_rys = eng.eri_tensor()
+    eng.close()
+    scale = np.maximum(1.0, np.abs(eri_rys))
+    assert np.max(np.abs(eri_os - eri_rys) / scale) < 1e-12
+
+
+def test_os_kernels_match_oracle_os(random_basis):
+    P = pfk()
+    eng = P.FockEngine(random_basis, engine="os")
+    eri_g = eng.eri_tensor()
+    eng.close()
+    ob = oracle.Basis(random_basis)
+    eri_o, _ = ob.eri_tensor(1e-10, oracle.OS)
+    assert np.max(np.abs(eri_g - eri_o) / np.maximum(1.0, np.abs(eri_o))) < 1e-10
+
+
+def test_engine_auto_runs_the_os_kernels(random_basis):
+    P = pfk()
+    eng = P.FockEngine(random_basis, engine="auto")
+    eri_auto = eng.eri_tensor()
+    eng.set_options(1e-10, "os")
+    eri_os = eng.eri_tensor()
+    eng.close()
+    assert np.array_equal(eri_auto, eri_os)
+
+
+def test_engine_switches_between_device_builds():
+    """Engine changes between captured device builds (each change drops the
+    captured graphs): every build stays within 1e-10 of the oracle's G."""
+    torch = pytest.importorskip("torch")
+    P = pfk()
+    mol, shells = P.shells_for(WATER, "cc-pvdz", basis_library())
+    ob = oracle.Basis(oracle.shells_for(oracle.Molecule(WATER), "cc-pvdz"))
+    eng = P.FockEngine(shells, engine="os")
+    nb = eng.nbasis
+    Pm = random_density(nb, seed=9)
+    eri_o, _ = ob.eri_tensor(1e-10, oracle.OS)
+    G_o = oracle.fock_rhf_tensor(eri_o, Pm)
+    dP = torch.tensor(Pm, device="cuda:0", dtype=torch.float64)
+    dG = torch.zeros_like(dP)
+    stream = torch.cuda.Stream()
+    for engine in ("os", "rys", "auto", "os"):
+        eng.set_options(1e-10, engine)
+        dG.fill_(float("nan"))
+        torch.cuda.synchronize()
+        eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), stream.cuda_stream)
+        stream.synchronize()
+        assert np.abs(dG.cpu().numpy() - G_o).max() < 1e-10
+    eng.close()
+
+
+def test_uhf_and_mixed_precision_on_os_kernels():
+    P = pfk()
+    mol, shells = P.shells_for(WATER, "6-31g**", basis_library())
+    ob = oracle.Basis(oracle.shells_for(oracle.Molecule(WATER), "6-31g**"))
+    eng = P.FockEngine(shells, engine="os")
+    nb = eng.nbasis
+    Pa, Pb = random_density(nb, seed=4), random_density(nb, seed=5)
+    eri_o, _ = ob.eri_tensor(1e-10, oracle.OS)
+    Ga_o, Gb_o = oracle.fock_uhf_tensor(eri_o, Pa, Pb)
+    Ga, Gb = eng.fock_uhf(Pa, Pb)
+    assert np.abs(Ga - Ga_o).max() < 1e-10 and np.abs(Gb - Gb_o).max() < 1e-10
+    G64 = eng.fock_rhf(Pa)
+    eng.set_options(1e-10, "os", "mixed", 1e-8)
+    Gmx = eng.fock_rhf(Pa)
+    eng.close()
+    assert np.abs(Gmx - G64).max() < 1e-7
+    assert abs(0.5 * np.sum(Pa * (Gmx - G64))) < 1e-6
