@@ -148,6 +148,46 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
  * roofline denominator of the integral kernels. */
 pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
+/* One-electron integrals of the basis: overlap S, kinetic energy T and
+ * nuclear attraction V (nbasis x nbasis, host buffers, symmetric), with
+ * point nuclei nuclei[4*natom] = (x, y, z in Bohr, charge Z).  Needs no
+ * context: runs on CUDA device `device` and returns when S, T, V are written.
+ * Counterpart of the reference's host-side Obara-Saika one-electron code
+ * (os.cpp:294-602), which the SCF setup calls before the first Fock build
+ * (H = T + V, scf.cpp:175-205). */
+pfk_status pfk_one_electron(const pfk_basis_desc *basis, int natom, const double *nuclei, double *S, double *T,
+                            double *V, int device);
+
+/* ---------------------------------------------------------------------------
+ * Learned initial guess: the network.  A multilayer perceptron
+ * (dims[0] -> dims[1] -> ... -> dims[nlayers], SiLU between layers, linear
+ * output) whose matrix products run on the tensor cores in BF16 with FP32
+ * accumulation, trained on the GPU with Adam on the mean squared error.  It
+ * has no counterpart in the reference: it predicts the atom-pair density
+ * blocks of the guess density that Planck's SCF takes like a ReadDensity
+ * guess (scf.cpp:206-240, 213-216).  Parameters are one FP32 vector: per
+ * layer the weight matrix W_l (dims[l] x dims[l+1], row-major, Z = H W + b)
+ * then the bias b_l.  Widths must be multiples of 8.  X, T, Y are device
+ * arrays of n rows (row-major FP32), n <= max_batch; the calls return when
+ * their results are written.
+ * ------------------------------------------------------------------------- */
+typedef struct pfk_mlp pfk_mlp;
+pfk_status pfk_mlp_create(int nlayers, const int *dims, int max_batch, int device, pfk_mlp **out);
+pfk_status pfk_mlp_destroy(pfk_mlp *m);
+const char *pfk_mlp_last_error(const pfk_mlp *m);
+long long pfk_mlp_param_count(const pfk_mlp *m);
+pfk_status pfk_mlp_set_params(pfk_mlp *m, const float *params);   /* host; resets Adam */
+pfk_status pfk_mlp_get_params(pfk_mlp *m, float *params);         /* host */
+/* Y = network(X). */
+pfk_status pfk_mlp_forward(pfk_mlp *m, const float *X, int n, float *Y, void *stream);
+/* Gradients (host vector in the parameter layout, may be NULL) and the loss
+ * mean((Y - T)^2) of one batch, without an update. */
+pfk_status pfk_mlp_gradients(pfk_mlp *m, const float *X, const float *T, int n, float *grads, double *loss,
+                             void *stream);
+/* One Adam step (beta 0.9, 0.999, eps 1e-8) with learning rate lr; loss as above. */
+pfk_status pfk_mlp_train_step(pfk_mlp *m, const float *X, const float *T, int n, float lr, double *loss,
+                              void *stream);
+
 /* Size of the device scratch array behind pfk_fock_rhf_noalloc: 64 MiB,
  * held by every GPU that loads the library until the process exits. */
 #define PFK_NOALLOC_SCRATCH_BYTES (64u << 20)

@@ -30,7 +30,9 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
            "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
-           "pfk_fock_rhf_noalloc"]
+           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
+           "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
+           "pfk_mlp_train_step"]
 
 _lib = None
 
@@ -76,6 +78,7 @@ def load_library(path=LIB_PATH):
     L.pfk_set_shard.argtypes = [vp, c_int, c_int]
     L.pfk_measure_fma_peak.argtypes = [c_int, ctypes.POINTER(c_dbl), ctypes.POINTER(c_dbl)]
     L.pfk_fock_rhf_noalloc.argtypes = [ctypes.POINTER(BasisDesc), vp, vp, c_dbl, vp]
+    L.pfk_one_electron.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, vp, vp, vp, c_int]
     _lib = L
     return L
 
@@ -200,6 +203,33 @@ class FockEngine:
         self._check(self.lib.pfk_set_shard(self.h, int(rank), int(nranks)))
 
 
+def _basis_desc(shells):
+    """(BasisDesc, arrays it points into) for a shells dict."""
+    keep = {k: np.ascontiguousarray(v) for k, v in shells.items()}
+    keep["L"] = np.ascontiguousarray(keep["L"], dtype=np.int32)
+    keep["nprim"] = np.ascontiguousarray(keep["nprim"], dtype=np.int32)
+    for k in ("center", "expo", "coef", "norm"):
+        keep[k] = _f64(keep[k])
+    desc = BasisDesc(len(keep["L"]), _p(keep["L"]), _p(keep["nprim"]), _p(keep["center"]), _p(keep["expo"]),
+                     _p(keep["coef"]), _p(keep["norm"]))
+    return desc, keep
+
+
+def one_electron(shells, coords, charges, device=0):
+    """Overlap S, kinetic T and nuclear attraction V (nb x nb) on the GPU for
+    point nuclei at `coords` (Bohr, natom x 3) with `charges` (pfk_one_electron)."""
+    L = load_library()
+    desc, keep = _basis_desc(shells)
+    nb = int(sum((int(l) + 1) * (int(l) + 2) // 2 for l in keep["L"]))
+    nuc = _f64(np.hstack([np.asarray(coords, dtype=np.float64).reshape(-1, 3),
+                          np.asarray(charges, dtype=np.float64).reshape(-1, 1)]))
+    S, T, V = (np.zeros((nb, nb)) for _ in range(3))
+    st = L.pfk_one_electron(ctypes.byref(desc), len(nuc), _p(nuc), _p(S), _p(T), _p(V), int(device))
+    if st != PFK_OK:
+        raise PfkError(st, L.pfk_last_error(None).decode())
+    return S, T, V
+
+
 def measure_fma_peak(device=0):
     """(FP64, FP32) FMA throughput of the device in TFLOP/s."""
     L = load_library()
@@ -253,3 +283,4 @@ def _compute_2e_fock_uhf(eng, Pa, Pb, nbasis, engine="os", tol_eri=1e-10, sym_op
     """(G_alpha, G_beta) (base.h:75-93)."""
     _prepare(eng, nbasis, engine, tol_eri, sym_ops)
     return eng.fock_uhf(Pa, Pb)
+from . import guess, mlp, scf  # noqa: E402,F401  (RHF driver and learned guess; import this package lazily)

@@ -24,23 +24,27 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC,
          "-I" + os.path.join(REPO, "include")]
 
 
-DEVICE_DEPS = ["pfk_device.cuh", "pfk_internal.h", "rys_table_data.inc"]
+DEVICE_DEPS = ["pfk_device.cuh", "pfk_internal.h", "rys_table_data.inc", "../../include/planck_fock.h"]
 DEPS = {
     "pfk_classes.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_os.cuh"],
     "pfk_setup.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_setup.h"],
     "pfk_api.cu": DEVICE_DEPS + ["pfk_setup.h", "../../include/planck_fock.h"],
+    "pfk_onee.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_os.cuh"],
+    "pfk_mlp.cu": ["../../include/planck_fock.h"],
 }
 
 
 # Class ranges per translation unit (class c = X(X+1)/2 + Y for bra pair
-# class X >= ket pair class Y): one unit per f-bra class, grouped below.
-CLASS_UNITS = [(0, 6), (6, 10), (10, 15), (15, 18), (18, 21)] + [(c, c + 1) for c in range(21, 55)]
+# class X >= ket pair class Y): one unit per class, so the 55 classes compile
+# in parallel.
+CLASS_UNITS = [(c, c + 1) for c in range(55)]
 
 
 def _units():
     units = [("pfk_classes.cu", f"classes_{b}_{e}.o", [f"-DPFK_CLASS_BEGIN={b}", f"-DPFK_CLASS_END={e}"])
              for b, e in reversed(CLASS_UNITS)]
-    units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", [])]
+    units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", []), ("pfk_onee.cu", "onee.o", []),
+              ("pfk_mlp.cu", "mlp.o", [])]
     return units
 
 

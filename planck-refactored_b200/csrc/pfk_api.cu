@@ -820,6 +820,33 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
     return PFK_OK;
 }
 
+pfk_status pfk_one_electron(const pfk_basis_desc *basis, int natom, const double *nuclei, double *S, double *T,
+                            double *V, int device)
+{
+    std::string why;
+    pfk_status vs = validate(basis, why);
+    if (vs != PFK_OK) {
+        g_last_error = "pfk_one_electron: " + why;
+        return vs;
+    }
+    if (natom < 0 || (natom > 0 && !nuclei) || !S || !T || !V) {
+        g_last_error = "pfk_one_electron: null output or nuclei pointer, or natom < 0";
+        return PFK_ERR_INVALID;
+    }
+    for (int c = 0; c < 4 * natom; ++c)
+        if (!std::isfinite(nuclei[c])) {
+            g_last_error = "pfk_one_electron: non-finite nuclear coordinate or charge";
+            return PFK_ERR_INVALID;
+        }
+    std::string what;
+    cudaError_t e = one_electron_run(basis, natom, nuclei, S, T, V, device, what);
+    if (e != cudaSuccess) {
+        g_last_error = "pfk_one_electron: " + what + ": " + cudaGetErrorString(e);
+        return PFK_ERR_CUDA;
+    }
+    return PFK_OK;
+}
+
 pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops)
 {
     cudaError_t e = measure_fma_peak(device, fp64_tflops, fp32_tflops);

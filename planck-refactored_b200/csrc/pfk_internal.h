@@ -1,8 +1,11 @@
 // pfk_internal.h -- shared host-side declarations of the Fock engine.
 #pragma once
+#include <string>
+
 #include <cuda_runtime.h>
 
 #include "pfk_device.cuh"
+#include "planck_fock.h"
 
 namespace pfk {
 
@@ -37,5 +40,10 @@ using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs 
 // units (each compiled for a range of classes).  A launcher called with
 // n < 0 only configures the current device for its kernels.
 extern ClassLauncher g_class_launchers[kQuartetClasses];
+
+// One-electron integrals S, T, V of a validated basis on `device` (pfk_onee.cu);
+// on failure `what` names the step.
+cudaError_t one_electron_run(const pfk_basis_desc *basis, int natom, const double *nuclei, double *S, double *T,
+                             double *V, int device, std::string &what);
 
 }  // namespace pfk

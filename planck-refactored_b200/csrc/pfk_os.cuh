@@ -50,17 +50,18 @@ __host__ __device__ constexpr double boys_series_coef(int M, int k)
     return (k % 2 ? -1.0 : 1.0) / (f * (2 * M + 2 * k + 1));
 }
 
-// Boys function F_m(T), m = 0..M (M <= 4).  T below TS: the Taylor series of
+// Boys function F_m(T), m = 0..M (M <= 6).  T below TS: the Taylor series of
 // F_M and downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1), which is
 // stable.  T >= TS: F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward
 // recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T); its error growth stays
-// below ~10x for m <= 4 at T >= 2 (and ~2x for m <= 1 at T >= 1).  Measured
-// against 40-digit values: max relative error 8e-15 (M = 4), 1e-15 (M <= 1).
+// below ~10x for m <= 4 at T >= 2 (~2x for m <= 1 at T >= 1; TS = 3 for
+// m = 5, 6).  Measured against 40-digit values: max relative error 1e-15
+// (M <= 1), 8e-15 (M = 4), 2e-14 (M = 6).
 template <int M>
 __device__ __forceinline__ void boys_fm(double T, double *F)
 {
-    constexpr double TS = M <= 1 ? 1.0 : 2.0;
-    constexpr int NT = M <= 1 ? 18 : 25;          // terms: last term < 1e-17 at T = TS
+    constexpr double TS = M <= 1 ? 1.0 : M <= 4 ? 2.0 : 3.0;
+    constexpr int NT = M <= 1 ? 18 : M <= 4 ? 25 : 32;   // terms: last term < 1e-17 at T = TS
     if (T < TS) {
         double s = boys_series_coef(M, NT - 1);
 #pragma unroll

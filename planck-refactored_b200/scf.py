@@ -1,0 +1,172 @@
+"""RHF driver around the GPU Fock build: the loop Planck's run_rhf runs
+(src/scf/scf.cpp:175-441), with the two-electron part from a FockEngine.
+
+Steps, as the reference takes them:
+  * symmetric orthogonaliser X = S^-1/2 (scf.cpp:15-20);
+  * default guess: eigenvectors of X^T H X, P = 2 C_occ C_occ^T
+    (scf.cpp:33-45, SCFGuess::HCore, types.h:329-347); a caller-supplied
+    density enters like the reference's ReadDensity guess (scf.cpp:213-216);
+  * per iteration F = H + G(P), E = 1/2 sum P (H + F) + E_nuc, Pulay DIIS over
+    the last 8 Fock matrices with error X^T (F P S - S P F) X
+    (types.h:759-837), diagonalisation of X^T F X, new P;
+  * converged when |dE| < 1e-10 and the rms and max of dP are below 1e-10,
+    not before the second iteration (scf.cpp:126-135); at most 50/100/200/300
+    iterations by basis size (types.h:356-363).
+
+Everything here is FP64 on the host, as the reference keeps DIIS and the
+diagonalisation.  Options beyond the reference:
+  * `incremental`: G(P_n) = G(P_{n-1}) + G(P_n - P_{n-1}) with the
+    difference-density build in FP32 (a second context whose whole quartet
+    list is on the FP32 path), and a full FP64 build every `full_every`
+    iterations and for the final energy;
+  * the learned-guess hook (guess.py) supplies P0 and the acceptance rule.
+"""
+import numpy as np
+import scipy.linalg as sla
+
+from .basis import ANGSTROM_TO_BOHR  # noqa: F401  (re-exported for callers building geometries)
+
+
+def nuclear_repulsion(coords, charges):
+    e = 0.0
+    n = len(charges)
+    for i in range(n):
+        for j in range(i):
+            e += charges[i] * charges[j] / np.linalg.norm(coords[i] - coords[j])
+    return e
+
+
+def max_cycles(nb):
+    """types.h:356-363"""
+    return 300 if nb > 1000 else 200 if nb > 500 else 100 if nb > 250 else 50
+
+
+def orthogonaliser(S):
+    s, U = np.linalg.eigh(S)
+    return (U * (1.0 / np.sqrt(s))) @ U.T
+
+
+def hcore_density(H, X, nocc):
+    _, Cp = np.linalg.eigh(X.T @ H @ X)
+    C = X @ Cp[:, :nocc]
+    return 2.0 * C @ C.T
+
+
+def _lstsq_pivoted(A, b):
+    """Least squares by column-pivoted QR with a relative rank cut-off of
+    n * eps * |R_00| (the solver the reference's DIIS uses, types.h:813)."""
+    Q, R, piv = sla.qr(A, pivoting=True)
+    d = np.abs(np.diag(R))
+    rank = int(np.count_nonzero(d > np.finfo(float).eps * len(d) * d[0]))
+    x = np.zeros(A.shape[1])
+    if rank:
+        x[piv[:rank]] = sla.solve_triangular(R[:rank, :rank], (Q.T @ b)[:rank])
+    return x
+
+
+class Pulay:
+    """DIIS over the last `depth` Fock matrices and error vectors."""
+
+    def __init__(self, depth=8):
+        self.depth, self.F, self.E = depth, [], []
+
+    def add(self, F, e):
+        self.F = (self.F + [F.copy()])[-self.depth:]
+        self.E = (self.E + [e.copy()])[-self.depth:]
+
+    def fock(self):
+        m = len(self.F)
+        if m < 2:
+            return self.F[-1]
+        B = -np.ones((m + 1, m + 1))
+        B[m, m] = 0.0
+        for i in range(m):
+            for j in range(i, m):
+                B[i, j] = B[j, i] = float(np.vdot(self.E[i], self.E[j]))
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        c = _lstsq_pivoted(B, rhs)
+        return sum(c[i] * self.F[i] for i in range(m))
+
+
+def first_energy(H, enuc, P, G):
+    """Energy of one Fock build on density P (the acceptance test of a guess)."""
+    F = H + G
+    return 0.5 * float(np.sum(P * (H + F))) + enuc
+
+
+def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8,
+        incremental=None, full_every=8):
+    """Run RHF to convergence.  engine: FockEngine (its fock_rhf gives
+    G = J - K/2).  P0: starting density (default: the core-Hamiltonian
+    guess); G0: G(P0) if the caller already built it (the guess hook does).
+    incremental: an optional second FockEngine on the same basis set to
+    mixed precision with an fp32_bound above every Schwarz bound, used for
+    the difference-density builds.  Returns a dict with energy, iterations,
+    converged, P, C, eps, history and the first-iteration energy."""
+    nb = H.shape[0]
+    X = orthogonaliser(S)
+    P = hcore_density(H, X, nocc) if P0 is None else np.array(P0, dtype=np.float64)
+    max_iter = max_iter or max_cycles(nb)
+    diis = Pulay(diis_depth)
+    E_prev, G, P_built, history, E_first = 0.0, None, None, [], None
+    for it in range(1, max_iter + 1):
+        if it == 1 and G0 is not None:
+            G = np.array(G0, dtype=np.float64)
+        elif incremental is not None and G is not None and (it - 1) % full_every:
+            G = G + incremental.fock_rhf(P - P_built)
+        else:
+            G = engine.fock_rhf(P)
+        P_built = P
+        F = H + G
+        E = 0.5 * float(np.sum(P * (H + F))) + enuc
+        if E_first is None:
+            E_first = E
+        diis.add(F, X.T @ (F @ P @ S - S @ P @ F) @ X)
+        eps, Cp = np.linalg.eigh(X.T @ diis.fock() @ X)
+        C = X @ Cp
+        Pn = 2.0 * C[:, :nocc] @ C[:, :nocc].T
+        dP = Pn - P
+        dE, dmax, drms = abs(E - E_prev), float(np.abs(dP).max()), float(np.sqrt(np.mean(dP * dP)))
+        history.append((it, E, dE, drms, dmax))
+        P, E_prev = Pn, E
+        if it > 1 and dE < tol_e and drms < tol_d and dmax < tol_d:
+            if incremental is not None:   # report the energy of a full build at the converged density
+                E_prev = first_energy(H, enuc, P, engine.fock_rhf(P))
+            return {"energy": E_prev, "iterations": it, "converged": True, "P": P, "C": C, "eps": eps,
+                    "history": history, "first_energy": E_first}
+    return {"energy": E_prev, "iterations": max_iter, "converged": False, "P": P, "C": C, "eps": eps,
+            "history": history, "first_energy": E_first}
+
+
+class System:
+    """A molecule on one GPU: basis shells, one-electron matrices from the
+    device (pfk_one_electron), nuclear repulsion and a FockEngine."""
+
+    def __init__(self, atoms, basis_name, library, device=0, engine="os", precision="fp64", fp32_bound=1e-8):
+        from . import FockEngine, one_electron, shells_for
+        self.mol, self.shells = shells_for(atoms, basis_name, library)
+        S, T, V = one_electron(self.shells, self.mol.coords, self.mol.Z, device)
+        self.S, self.H = S, T + V
+        self.enuc = nuclear_repulsion(self.mol.coords, self.mol.Z)
+        self.nocc = self.mol.nelectron() // 2
+        self.engine = FockEngine(self.shells, device=device, engine=engine, precision=precision,
+                                 fp32_bound=fp32_bound)
+        self.device = device
+        self._incr = None
+
+    def incremental_engine(self):
+        if self._incr is None:
+            from . import FockEngine
+            self._incr = FockEngine(self.shells, device=self.device, engine=self.engine.engine, precision="mixed",
+                                    fp32_bound=1e300)
+        return self._incr
+
+    def run(self, P0=None, incremental=False, **kw):
+        return rhf(self.engine, self.H, self.S, self.enuc, self.nocc, P0=P0,
+                   incremental=self.incremental_engine() if incremental else None, **kw)
+
+    def close(self):
+        self.engine.close()
+        if self._incr is not None:
+            self._incr.close()

@@ -4,6 +4,9 @@
     seeded rigid rotations and +-0.2 Angstrom jitter of the experimental
     monomer (O (0,0,0.1173), H (0,+-0.7572,-0.4692) Angstrom);
   * alkane: all-trans CnH2n+2 with seeded noise;
+  * alkane_conformer: seeded linear or branched CnH2n+2 conformers with
+    bond, angle and torsion noise (the learned-guess training and
+    evaluation sets);
   * random_shells: shells drawn like the ERI class microbenchmark
     (exponents log-uniform in [0.05, 1e4], contraction depth 1..6,
     coefficients uniform in (0, 1], reference normalisation).
@@ -63,6 +66,112 @@ def alkane(nc, seed=3, noise=0.03):
     for a in atoms:
         out.append([a[0], *(np.array(a[1:], dtype=float) + rng.uniform(-noise, noise, 3))])
     return out
+
+
+def _unit(v):
+    return v / np.linalg.norm(v)
+
+
+def _rotate(v, axis, ang):
+    """Rodrigues rotation of v about unit `axis` by `ang` radians."""
+    return v * np.cos(ang) + np.cross(axis, v) * np.sin(ang) + axis * np.dot(axis, v) * (1.0 - np.cos(ang))
+
+
+def alkane_conformer(nc, seed, branched=None, bond_noise=0.05, angle_noise_deg=5.0):
+    """A seeded conformer of an acyclic alkane CnH2n+2, as [symbol, x, y, z]
+    rows in Angstrom.
+
+    Skeleton: linear when `branched` is False; otherwise every new carbon
+    bonds to a random earlier carbon with fewer than three carbon neighbours
+    (or four for a quaternary centre, with small probability), so both linear
+    and branched isomers occur (branched=None draws the choice).  Geometry:
+    C-C 1.53 and C-H 1.09 Angstrom each with uniform +-bond_noise, bond
+    angles tetrahedral with uniform +-angle_noise_deg, and a random torsion
+    about every C-C bond: the substituents take the three staggered
+    positions (60, 180, 300 degrees from a substituent of the neighbouring
+    carbon, all shifted by one uniform +-20 degrees) in random order, so each
+    bond is a random trans/gauche rotamer.  Conformers whose non-bonded atoms
+    come closer than 1.7 Angstrom (C-C), 1.4 (C-H) or 1.2 (H-H) are redrawn."""
+    rng = np.random.default_rng(seed)
+    if branched is None:
+        branched = bool(rng.integers(0, 2)) and nc >= 4
+    tet = np.deg2rad(109.4712)
+
+    def too_close(x, sym, placed, skip):
+        for k, (s2, y) in enumerate(placed):
+            if k in skip:
+                continue
+            lim = 1.7 if sym == s2 == "C" else 1.2 if sym == s2 == "H" else 1.4
+            if np.linalg.norm(x - y) < lim:
+                return True
+        return False
+
+    for _attempt in range(100):
+        parent = [-1]
+        nbr = [[] for _ in range(nc)]
+        for c in range(1, nc):
+            if not branched:
+                p = c - 1
+            else:
+                cands = [q for q in range(c) if len(nbr[q]) < (4 if rng.random() < 0.1 else 3)]
+                p = int(rng.choice(cands)) if cands else c - 1
+            parent.append(p)
+            nbr[p].append(c)
+            nbr[c].append(p)
+        # placed atoms as (symbol, position); carbons keep their index c in slot[c]
+        placed, slot, hydrogens = [("C", np.zeros(3))], {0: 0}, []
+        dirs = {}
+        order = [0]
+        ok = True
+        while order and ok:
+            c = order.pop(0)
+            children = [x for x in nbr[c] if x != parent[c]]
+            for _try in range(40):
+                if c == 0:
+                    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+                    cand = [_unit(q @ v) for v in (np.array([1, 1, 1.0]), np.array([1, -1, -1.0]),
+                                                   np.array([-1, 1, -1.0]), np.array([-1, -1, 1.0]))]
+                    cand = [cand[k] for k in rng.permutation(4)]
+                else:
+                    pc = placed[slot[c]][1]
+                    u = _unit(placed[slot[parent[c]]][1] - pc)   # towards the parent
+                    # dihedrals are measured from another substituent of the parent
+                    ref = next(d for d in dirs[parent[c]] if np.dot(d, -u) < 0.9)
+                    r = _unit(ref - np.dot(ref, u) * u)
+                    w = np.cross(u, r)
+                    # staggered positions (60, 180, 300 degrees, all +-20) in
+                    # random order: which substituent is trans or gauche is random
+                    phi0 = np.deg2rad(60.0 + rng.uniform(-20.0, 20.0))
+                    cand = []
+                    for k in rng.permutation(3):
+                        ang = tet + np.deg2rad(rng.uniform(-angle_noise_deg, angle_noise_deg))
+                        phi = phi0 + 2 * np.pi * k / 3
+                        cand.append(_unit(np.cos(ang) * u + np.sin(ang) * (np.cos(phi) * r + np.sin(phi) * w)))
+                pc = placed[slot[c]][1]
+                new = []
+                for k, d in enumerate(cand):
+                    sym = "C" if k < len(children) else "H"
+                    new.append((sym, pc + d * ((1.53 if sym == "C" else 1.09) + rng.uniform(-bond_noise, bond_noise))))
+                # new substituents against every placed atom except this carbon
+                # and its parent (bonded or geminal by construction)
+                skip = {slot[c]} | ({slot[parent[c]]} if c else set())
+                if not any(too_close(x, sym, placed, skip) for sym, x in new):
+                    break
+            else:
+                ok = False
+                break
+            dirs[c] = cand
+            for k, (sym, x) in enumerate(new):
+                placed.append((sym, x))
+                if sym == "C":
+                    slot[children[k]] = len(placed) - 1
+                    order.append(children[k])
+                else:
+                    hydrogens.append(x)
+        if ok:
+            return [["C", *map(float, placed[slot[c]][1])] for c in range(nc)] + \
+                   [["H", *map(float, x)] for x in hydrogens]
+    raise RuntimeError(f"no clash-free conformer for C{nc} (seed {seed})")
 
 
 def random_shells(nshell, lmax=3, seed=11, box=10.0):

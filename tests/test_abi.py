@@ -16,7 +16,7 @@ HEADER = os.path.join(REPO, "include", "planck_fock.h")
 
 def declared_symbols():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:pfk_status|int|const char \*)\s*(pfk_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:pfk_status|int|long long|const char \*)\s*(pfk_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():

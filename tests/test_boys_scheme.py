@@ -1,8 +1,8 @@
 """The Boys-function scheme of the Obara-Saika kernels (CPU test).
 
-boys_fm<M> in csrc/pfk_os.cuh evaluates F_0..F_M (M <= 4) as follows:
-  * T below TS (1 for M <= 1, 2 otherwise): the Taylor series of F_M,
-    sum_k (-T)^k / (k! (2M+2k+1)), with 18 (M <= 1) or 25 terms, then the
+boys_fm<M> in csrc/pfk_os.cuh evaluates F_0..F_M (M <= 6) as follows:
+  * T below TS (1 for M <= 1, 2 for M <= 4, 3 above): the Taylor series of
+    F_M, sum_k (-T)^k / (k! (2M+2k+1)), with 18, 25 or 32 terms, then the
     downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1);
   * otherwise F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward recursion
     F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
@@ -24,7 +24,7 @@ def _coef(M, k):
 
 
 def boys_scheme(M, T):
-    TS, NT = (1.0, 18) if M <= 1 else (2.0, 25)
+    TS, NT = (1.0, 18) if M <= 1 else (2.0, 25) if M <= 4 else (3.0, 32)
     F = [0.0] * (M + 1)
     if T < TS:
         s = _coef(M, NT - 1)
@@ -52,7 +52,8 @@ def boys_exact(m, T):
         return mpmath.gammainc(m + mpmath.mpf(1) / 2, 0, T) / (2 * T ** (m + mpmath.mpf(1) / 2))
 
 
-@pytest.mark.parametrize("M,bound", [(0, 1e-15), (1, 2e-15), (2, 4e-15), (3, 8e-15), (4, 2e-14)])
+@pytest.mark.parametrize("M,bound", [(0, 1e-15), (1, 2e-15), (2, 4e-15), (3, 8e-15), (4, 2e-14), (5, 2e-14),
+                                     (6, 4e-14)])
 def test_boys_scheme_relative_error(M, bound):
     rng = np.random.default_rng(M)
     Ts = np.concatenate([rng.uniform(0, 3, 150), rng.uniform(0, 80, 150), np.logspace(-14, 3, 40),

@@ -1,0 +1,67 @@
+"""The learned-guess hook end to end (GPU tests).
+
+(a) A small model trained here on the GPU (48 conformers of C1-C6, through
+    the same generate/train code as the shipped model) drives the hook:
+    the purified guess has the right electron count and idempotency, and the
+    SCF started from whatever the hook chooses converges to the energy of
+    the default-guess SCF within 1e-8 Eh.
+(b) The shipped model (data/guess_model_631gs.npz, trained on 4096
+    conformers of C1-C12 by guess_train.py) on held-out conformers of
+    C8-C12: fewer SCF iterations than the default core-Hamiltonian guess,
+    same converged energies within 1e-8 Eh."""
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+from helpers import basis_library, pfk
+
+pytestmark = pytest.mark.gpu
+
+MODEL = os.path.join(os.path.dirname(__file__), "..", "planck-refactored_b200", "data", "guess_model_631gs.npz")
+
+
+def _trainer():
+    pfk()
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "planck-refactored_b200"))
+    return importlib.import_module("guess_train")
+
+
+def test_hook_with_a_small_trained_model(tmp_path):
+    P = pfk()
+    T = _trainer()
+    samples, info = T.generate(48, log=None)
+    assert info["molecules"] == 48
+    model = P.guess.GuessModel("6-31g*", seed=1)
+    P.guess.train(model, samples, epochs=8, lr=1e-3, batch=256)
+    path = os.path.join(tmp_path, "m.npz")
+    model.save(path)
+    model.close()
+    model = P.guess.GuessModel.load(path)
+    lib = basis_library()
+    for i in range(3):
+        nc, atoms = T.conformer(i, 3, 6, 2_000_000)
+        sysm = P.scf.System(atoms, "6-31g*", lib)
+        Pl = P.guess.predict_density(model, sysm)
+        S = sysm.S
+        assert abs(np.trace(Pl @ S) - 2 * sysm.nocc) < 1e-8
+        assert np.allclose(Pl @ S @ Pl, 2 * Pl, atol=1e-8)
+        r_d = sysm.run()
+        P0, G0, hook = P.guess.choose(model, sysm)
+        r_l = sysm.run(P0=P0, G0=G0)
+        sysm.close()
+        assert r_d["converged"] and r_l["converged"]
+        assert abs(r_l["energy"] - r_d["energy"]) < 1e-8
+        assert hook["E_first_learned"] == hook["E_first_learned"]   # finite
+    model.close()
+
+
+def test_shipped_model_reduces_iterations():
+    T = _trainer()
+    assert os.path.exists(MODEL), "the trained guess model is missing"
+    res = T.evaluate(MODEL, 8, lo=8, hi=12)
+    assert res["all_converged"]
+    assert res["max_abs_dE_Eh"] < 1e-8
+    assert res["mean_iterations_learned"] < res["mean_iterations_default"]
