@@ -27,6 +27,10 @@ template <typename T>
 struct DevBuf {
     T *p = nullptr;
     size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }   // the temporaries of list building are freed on every path
     cudaError_t alloc(size_t count)
     {
         release();

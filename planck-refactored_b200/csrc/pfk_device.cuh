@@ -180,9 +180,11 @@ __device__ __forceinline__ void rys_root_one(double T, int r, double &u, double 
 // ---------------------------------------------------------------------------
 // Per-axis 2D integrals of one root (rys.cpp:250-280 recurrence), then the
 // A->B and C->D transfers on that axis (rys.cpp:293-363 applied per axis):
-// out[((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d] = I_axis(a, b, c, d).
+// out[a*AST + b*BST + c*(LD+1) + d] = I_axis(a, b, c, d).  The default strides
+// pack the table densely; shared-memory tables pass padded strides so that
+// lanes reading different a (or a, b) slices hit different banks.
 // ---------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, int BST = (LC + 1) * (LD + 1), int AST = (LB + 1) * BST>
 __device__ __forceinline__ void axis_table(R C00, R D00, R B00, R B10, R B01, R AB, R CD, R scale,
                                            R *__restrict__ out)
 {
@@ -230,8 +232,7 @@ __device__ __forceinline__ void axis_table(R C00, R D00, R B00, R B10, R B01, R 
 #pragma unroll
             for (int c = 0; c <= LC; ++c)
 #pragma unroll
-                for (int d = 0; d <= LD; ++d)
-                    out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = H[c][d];
+                for (int d = 0; d <= LD; ++d) out[a * AST + b * BST + c * (LD + 1) + d] = H[c][d];
         }
 }
 

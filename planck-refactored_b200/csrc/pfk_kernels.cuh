@@ -523,7 +523,13 @@ struct SplitShape {
     static constexpr int TEAM = pow2ceil(GROUP) < 4 ? 4 : pow2ceil(GROUP);
     static constexpr int TEAMS = 128 / TEAM;
     static constexpr int SB = LEVEL == 1 ? (LB + 1) * (LC + 1) * (LD + 1) : (LC + 1) * (LD + 1);
-    static constexpr int TABLE = S::NR * 3 * S::NI;
+    // table strides: a slice a (LEVEL 1) or (a, b) (LEVEL 2) is read by
+    // different lanes at once, so slices start an odd number of doubles
+    // apart (no two of them on the same shared-memory bank pair)
+    static constexpr int BST = LEVEL == 2 ? (LC + 1) * (LD + 1) + ((LC + 1) * (LD + 1) + 1) % 2 : (LC + 1) * (LD + 1);
+    static constexpr int AST = LEVEL == 1 ? (LB + 1) * BST + ((LB + 1) * BST + 1) % 2 : (LB + 1) * BST;
+    static constexpr int NIP = (LA + 1) * AST;                 // padded table per (root, axis)
+    static constexpr int TABLE = S::NR * 3 * NIP + (S::NR * 3 * NIP + 1) % 2;
     static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
     static constexpr bool OK = TEAM <= 128 && M <= 64;
 };
@@ -558,11 +564,11 @@ __device__ __forceinline__ int cart_l_axis(int i, int axis)
 }
 
 template <int LA, int LB, int LC, int LD, int NK>
-__global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
+__global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
 {
     using S = ClassShape<LA, LB, LC, LD>;
     using SS = SplitShape<LA, LB, LC, LD>;
-    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
+    constexpr int NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR;
     constexpr int TEAM = SS::TEAM, LEVEL = SS::LEVEL, NBT = SS::NBT, SB = SS::SB, M = SS::M;
     extern __shared__ double smem[];
     const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
@@ -570,7 +576,7 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
     if (t >= nq) return;   // whole teams leave together; barriers are per team
     const unsigned mask = TEAM >= 32 ? 0xffffffffu
                                      : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
-    double *g = smem + team * SS::TABLE;   // g[r][axis][NI]
+    double *g = smem + team * SS::TABLE;   // g[r][axis][NIP]
 
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
@@ -584,7 +590,7 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         const int la = cart_l_axis<LA>(ia, x);
-        base[x] = LEVEL == 1 ? la * SB : (la * (LB + 1) + cart_l_axis<LB>(ib0, x)) * SB;
+        base[x] = LEVEL == 1 ? la * SS::AST : la * SS::AST + cart_l_axis<LB>(ib0, x) * SS::BST;
     }
 
     double acc[M];
@@ -610,7 +616,8 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
                 if (axis == 0) { C00 = p.PAx + ur * s.WPx; D00 = q.PAx + ur * s.WQx; AB = pb.ABx; CD = pk.ABx; scale = wr * s.pref; }
                 else if (axis == 1) { C00 = p.PAy + ur * s.WPy; D00 = q.PAy + ur * s.WQy; AB = pb.ABy; CD = pk.ABy; }
                 else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
-                axis_table<LA, LB, LC, LD, double>(C00, D00, B00, B10, B01, AB, CD, scale, g + (r * 3 + axis) * NI);
+                axis_table<LA, LB, LC, LD, double, SS::BST, SS::AST>(C00, D00, B00, B10, B01, AB, CD, scale,
+                                                                       g + (r * 3 + axis) * SS::NIP);
             }
             split_sync<TEAM>(mask, team);
             if (owner) {
@@ -619,9 +626,9 @@ __global__ void __launch_bounds__(128) eri_split_kernel(const uint2 *__restrict_
                     double tx[SB], ty[SB], tz[SB];
 #pragma unroll
                     for (int e = 0; e < SB; ++e) {
-                        tx[e] = g[(r * 3 + 0) * NI + base[0] + e];
-                        ty[e] = g[(r * 3 + 1) * NI + base[1] + e];
-                        tz[e] = g[(r * 3 + 2) * NI + base[2] + e];
+                        tx[e] = g[(r * 3 + 0) * SS::NIP + base[0] + e];
+                        ty[e] = g[(r * 3 + 1) * SS::NIP + base[1] + e];
+                        tz[e] = g[(r * 3 + 2) * SS::NIP + base[2] + e];
                     }
 #pragma unroll
                     for (int bl = 0; bl < NBT; ++bl)

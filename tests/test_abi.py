@@ -169,3 +169,22 @@ def test_device_rys_table_reproduces_boys_moments():
                 uo, wo = oracle.rys_roots(n, T)
                 np.testing.assert_allclose(u, uo, rtol=1e-12, atol=1e-15)
                 np.testing.assert_allclose(w, wo, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_contexts_do_not_leak_device_memory():
+    """Building the screened lists allocates temporaries; 200 create/destroy
+    cycles must leave the device's free memory where it was (within 8 MiB)."""
+    torch = pytest.importorskip("torch")
+    P = pfk()
+    mol, shells = P.shells_for(WATER, "6-31g**", basis_library())
+    for _ in range(5):
+        P.FockEngine(shells).close()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(200):
+        eng = P.FockEngine(shells)
+        eng.set_options(1e-9, "os")       # a second list build
+        eng.close()
+    torch.cuda.synchronize()
+    assert free0 - torch.cuda.mem_get_info()[0] < 8 << 20

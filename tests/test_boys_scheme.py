@@ -4,8 +4,9 @@ boys_fm<M> in csrc/pfk_os.cuh evaluates F_0..F_M (M <= 6) as follows:
   * T below TS (1 for M <= 1, 2 for M <= 4, 3 above): the Taylor series of
     F_M, sum_k (-T)^k / (k! (2M+2k+1)), with 18, 25 or 32 terms, then the
     downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1);
-  * otherwise F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward recursion
-    F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
+  * up to TA (50 for M <= 4, 60 above) F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T
+    and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T);
+  * above TA the large-T limit F_0 = sqrt(pi/4T), F_{m+1} = (2m+1) F_m / (2T).
 This test restates that scheme in double precision with the C library's erf
 and exp and checks it against 40-digit Boys values.  The scheme's parameters
 (thresholds, term counts) are what the device code uses.  The device's erf
@@ -34,13 +35,19 @@ def boys_scheme(M, T):
         e = math.exp(-T)
         for m in range(M - 1, -1, -1):
             F[m] = (2.0 * T * F[m + 1] + e) * (1.0 / (2 * m + 1))
-    else:
+    elif T < (50.0 if M <= 4 else 60.0):
         ist = 1.0 / math.sqrt(T)
         F[0] = 0.88622692545275801365 * math.erf(T * ist) * ist
         e = math.exp(-T)
         h = 0.5 * ist * ist
         for m in range(M):
             F[m + 1] = ((2 * m + 1) * F[m] - e) * h
+    else:
+        ist = 1.0 / math.sqrt(T)
+        F[0] = 0.88622692545275801365 * ist
+        h = 0.5 * ist * ist
+        for m in range(M):
+            F[m + 1] = (2 * m + 1) * h * F[m]
     return F
 
 
@@ -56,8 +63,10 @@ def boys_exact(m, T):
                                      (6, 4e-14)])
 def test_boys_scheme_relative_error(M, bound):
     rng = np.random.default_rng(M)
-    Ts = np.concatenate([rng.uniform(0, 3, 150), rng.uniform(0, 80, 150), np.logspace(-14, 3, 40),
-                         [0.0, 0.999999999, 1.0, 1.000000001, 1.999999999, 2.0, 2.000000001]])
+    Ts = np.concatenate([rng.uniform(0, 3, 150), rng.uniform(0, 80, 150), rng.uniform(45, 65, 60),
+                         np.logspace(-14, 3, 40),
+                         [0.0, 0.999999999, 1.0, 1.000000001, 1.999999999, 2.0, 2.000000001, 49.999999, 50.0,
+                          59.999999, 60.0]])
     worst = 0.0
     for T in Ts:
         F = boys_scheme(M, float(T))
