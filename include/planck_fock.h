@@ -142,6 +142,15 @@ pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_
  * all-reduce. */
 pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
 
+/* Density screening for builds on a difference density (incremental SCF):
+ * with dtol > 0, every later build of this context first takes the largest
+ * |P| of each shell-pair block over the densities it is given, and skips
+ * every shell quartet whose Schwarz bound qmax(ab) qmax(cd) times the
+ * largest of its six density blocks is below dtol.  A build on a full
+ * density does not want this (its result would no longer be the
+ * reference's); dtol = 0 turns it off.  Not in the reference. */
+pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol);
+
 /* Measurement helper: sustained FP64 and FP32 fused-multiply-add throughput
  * of `device` in TFLOP/s (2 flops per FMA), from a register-resident FMA
  * loop over all SMs, timed with CUDA events.  The FP64 figure is the

@@ -30,7 +30,7 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
            "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
-           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
+           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step"]
 
@@ -79,6 +79,7 @@ def load_library(path=LIB_PATH):
     L.pfk_measure_fma_peak.argtypes = [c_int, ctypes.POINTER(c_dbl), ctypes.POINTER(c_dbl)]
     L.pfk_fock_rhf_noalloc.argtypes = [ctypes.POINTER(BasisDesc), vp, vp, c_dbl, vp]
     L.pfk_one_electron.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, vp, vp, vp, c_int]
+    L.pfk_set_density_screening.argtypes = [vp, c_dbl]
     _lib = L
     return L
 
@@ -201,6 +202,11 @@ class FockEngine:
 
     def set_shard(self, rank, nranks):
         self._check(self.lib.pfk_set_shard(self.h, int(rank), int(nranks)))
+
+    def set_density_screening(self, dtol):
+        """Skip shell quartets whose Schwarz bound times the largest density
+        block they touch is below dtol (for difference-density builds; 0 off)."""
+        self._check(self.lib.pfk_set_density_screening(self.h, float(dtol)))
 
 
 def _basis_desc(shells):

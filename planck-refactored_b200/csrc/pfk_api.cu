@@ -63,6 +63,9 @@ struct pfk_ctx {
 
     int nshell = 0, nb = 0;
     std::vector<int> L, bf_off;
+    DevBuf<int> d_shell_bf, d_shell_nbf;      // per shell: first basis function, function count
+    double dscreen_tol = 0.0;                 // density screening threshold (0: off)
+    DevBuf<float> d_Dsh;                      // per shell-pair block max |P| (nb x nb, block corners)
 
     int npairs = 0;
     std::vector<PairInfo> pairs;
@@ -405,6 +408,12 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         if (K1) PFK_CK(cudaMemsetAsync(K1, 0, sizeof(double) * nb2, st));
     }
     JKArgs a{};
+    if (ctx->dscreen_tol > 0.0 && !eri_out) {
+        PFK_CK(shell_block_max(ctx->nshell, ctx->d_shell_bf.p, ctx->d_shell_nbf.p, Pj, Pk0 != Pj ? Pk0 : nullptr, Pk1,
+                               ctx->nb, ctx->d_Dsh.p, st));
+        a.Dsh = ctx->d_Dsh.p;
+        a.dtol = ctx->dscreen_tol;
+    }
     a.pairs = ctx->d_pairs.p;
     a.prims = ctx->d_prims.p;
     a.Qao = ctx->d_Q.p;
@@ -592,6 +601,9 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
         ctx->d_cls_kpref[x].release();
     }
     ctx->d_quart.release();
+    ctx->d_shell_bf.release();
+    ctx->d_shell_nbf.release();
+    ctx->d_Dsh.release();
     for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
         b->release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -811,6 +823,26 @@ pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_
         if (quartets55) quartets55[c] = ctx->q_cnt[c] + ctx->q32_cnt[c];
         if (prim_quartets55) prim_quartets55[c] = ctx->prim_cnt[c];
     }
+    return PFK_OK;
+}
+
+pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!(dtol >= 0.0) || !std::isfinite(dtol)) return ctx->fail(PFK_ERR_INVALID, "dtol must be finite and >= 0");
+    cudaSetDevice(ctx->device);
+    if (dtol > 0.0 && !ctx->d_Dsh.p) {
+        std::vector<int> nbf(ctx->nshell);
+        for (int s = 0; s < ctx->nshell; ++s) nbf[s] = ncart(ctx->L[s]);
+        PFK_CK(ctx->d_shell_bf.alloc(ctx->nshell));
+        PFK_CK(ctx->d_shell_nbf.alloc(ctx->nshell));
+        PFK_CK(cudaMemcpy(ctx->d_shell_bf.p, ctx->bf_off.data(), sizeof(int) * ctx->nshell, cudaMemcpyHostToDevice));
+        PFK_CK(cudaMemcpy(ctx->d_shell_nbf.p, nbf.data(), sizeof(int) * ctx->nshell, cudaMemcpyHostToDevice));
+        PFK_CK(ctx->d_Dsh.alloc((size_t)ctx->nb * ctx->nb));
+        PFK_CK(cudaMemset(ctx->d_Dsh.p, 0, sizeof(float) * (size_t)ctx->nb * ctx->nb));
+    }
+    if (dtol != ctx->dscreen_tol) drop_graphs(ctx);   // captured builds hold the old setting
+    ctx->dscreen_tol = dtol;
     return PFK_OK;
 }
 

@@ -107,6 +107,12 @@ struct JKArgs {
     // this launch evaluates quartets[t * qstride + qoffset], t < nq (one
     // shard of a list split across GPUs; 1 and 0 for the whole list)
     int qstride, qoffset;
+    // density screening (builds on a difference density): when Dsh is set,
+    // a shell quartet is skipped if qmax(bra) qmax(ket) max|D| < dtol, with
+    // Dsh[first bf of shell 1 * nb + first bf of shell 2] = max |P| over
+    // that shell-pair block of every density of the build
+    const float *__restrict__ Dsh;
+    double dtol;
 };
 
 // ---------------------------------------------------------------------------

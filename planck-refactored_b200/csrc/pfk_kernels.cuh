@@ -44,6 +44,20 @@ struct ClassShape {
     }
 };
 
+// Density screening of a whole shell quartet: every J and K contribution
+// is a density block (kl, ij, jl, il, jk or ik) times integrals bounded by
+// qmax(ij) qmax(kl).
+__device__ __forceinline__ bool density_negligible(const PairInfo &pb, const PairInfo &pk, const JKArgs &a)
+{
+    if (!a.Dsh) return false;
+    const size_t nb = a.nb;
+    const int i = pb.bf_a, j = pb.bf_b, k = pk.bf_a, l = pk.bf_b;
+    const float d = fmaxf(fmaxf(fmaxf(__ldg(a.Dsh + k * nb + l), __ldg(a.Dsh + i * nb + j)),
+                                fmaxf(__ldg(a.Dsh + j * nb + l), __ldg(a.Dsh + i * nb + l))),
+                          fmaxf(__ldg(a.Dsh + j * nb + k), __ldg(a.Dsh + i * nb + k)));
+    return pb.qmax * pk.qmax * (double)d < a.dtol;
+}
+
 // Canonical-quartet bookkeeping for one Cartesian component quartet.
 // Returns the weight s (0 when the component is a duplicate or screened out).
 __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, bool same_bk, int ia, int ib,
@@ -272,6 +286,7 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
+    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
 
     R acc[NA * NB * NC * ND];
 #pragma unroll
@@ -360,6 +375,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
+    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
 
     int off[KPT];
     double acc[KPT];
@@ -581,6 +597,7 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
+    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
     const bool owner = lane < SS::GROUP;
     const int gi = owner ? lane : 0;
     const int ia = LEVEL == 1 ? gi : gi / NB;

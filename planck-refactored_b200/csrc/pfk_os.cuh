@@ -50,6 +50,21 @@ __host__ __device__ constexpr double boys_series_coef(int M, int k)
     return (k % 2 ? -1.0 : 1.0) / (f * (2 * M + 2 * k + 1));
 }
 
+// The series coefficients as a constant-memory table: the FMAs of the series
+// then read them as constant-bank operands instead of materialising each
+// 64-bit literal in registers.
+struct BoysSeriesTable {
+    double c[7][32];
+};
+__host__ __device__ constexpr BoysSeriesTable make_boys_series_table()
+{
+    BoysSeriesTable t{};
+    for (int M = 0; M < 7; ++M)
+        for (int k = 0; k < 32; ++k) t.c[M][k] = boys_series_coef(M, k);
+    return t;
+}
+static __constant__ const BoysSeriesTable kBoysSeries = make_boys_series_table();
+
 // Boys function F_m(T), m = 0..M (M <= 6).  T below TS: the Taylor series of
 // F_M and downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1), which is
 // stable.  T >= TS: F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward
@@ -66,9 +81,9 @@ __device__ __forceinline__ void boys_fm(double T, double *F)
     constexpr int NT = M <= 1 ? 18 : M <= 4 ? 25 : 32;   // terms: last term < 1e-17 at T = TS
     constexpr double TA = M <= 4 ? 50.0 : 60.0;           // large-T limit from here on
     if (T < TS) {
-        double s = boys_series_coef(M, NT - 1);
+        double s = kBoysSeries.c[M][NT - 1];
 #pragma unroll
-        for (int k = NT - 2; k >= 0; --k) s = fma(s, T, boys_series_coef(M, k));
+        for (int k = NT - 2; k >= 0; --k) s = fma(s, T, kBoysSeries.c[M][k]);
         F[M] = s;
         if constexpr (M > 0) {
             const double e = exp(-T);
@@ -328,6 +343,7 @@ __global__ void __launch_bounds__(128) eri_os_kernel(const uint2 *__restrict__ q
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
+    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
 
     R acc[O::NACC];
 #pragma unroll

@@ -272,6 +272,33 @@ __global__ void __launch_bounds__(256) fma_chain_kernel(T *out, int iters, T a, 
     out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
 }
 
+__global__ void shell_block_max_kernel(int nshell, const int *__restrict__ bf_off, const int *__restrict__ nbf,
+                                       const double *__restrict__ P0, const double *__restrict__ P1,
+                                       const double *__restrict__ P2, int nb, float *__restrict__ D)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nshell * nshell) return;
+    const int s1 = (int)(t / nshell), s2 = (int)(t % nshell);
+    const int i0 = bf_off[s1], j0 = bf_off[s2], ni = nbf[s1], nj = nbf[s2];
+    double m = 0.0;
+    for (int i = 0; i < ni; ++i)
+        for (int j = 0; j < nj; ++j) {
+            const size_t k = (size_t)(i0 + i) * nb + j0 + j;
+            m = fmax(m, fabs(P0[k]));
+            if (P1) m = fmax(m, fabs(P1[k]));
+            if (P2) m = fmax(m, fabs(P2[k]));
+        }
+    D[(size_t)i0 * nb + j0] = __double2float_ru(m);
+}
+
+cudaError_t shell_block_max(int nshell, const int *bf_off, const int *nbf, const double *P0, const double *P1,
+                            const double *P2, int nb, float *D, cudaStream_t st)
+{
+    const long long n = (long long)nshell * nshell;
+    shell_block_max_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nshell, bf_off, nbf, P0, P1, P2, nb, D);
+    return cudaGetLastError();
+}
+
 template <typename T>
 static cudaError_t time_fma(int device, double *tflops)
 {

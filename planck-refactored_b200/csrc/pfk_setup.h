@@ -23,6 +23,10 @@ cudaError_t bra_work(const int *idX, int nX, int diag, const long long *cnt_hi, 
                      const long long *kprefY, const PairInfo *pairs, long long *work_hi, long long *work_lo,
                      cudaStream_t st);
 cudaError_t measure_fma_peak(int device, double *fp64, double *fp32);
+// D[first bf(s1) * nb + first bf(s2)] = max |P| over the (s1, s2) block of
+// every non-null density P0..P2 (rounded up to FP32), for density screening.
+cudaError_t shell_block_max(int nshell, const int *bf_off, const int *nbf, const double *P0, const double *P1,
+                            const double *P2, int nb, float *D, cudaStream_t st);
 cudaError_t sort_quartets(uint2 *q, long long n, const PairInfo *pairs, unsigned *keys_a, unsigned *keys_b,
                           uint2 *vals_b, void *temp, size_t &temp_bytes, cudaStream_t st);
 

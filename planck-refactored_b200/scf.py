@@ -17,8 +17,11 @@ Everything here is FP64 on the host, as the reference keeps DIIS and the
 diagonalisation.  Options beyond the reference:
   * `incremental`: G(P_n) = G(P_{n-1}) + G(P_n - P_{n-1}) with the
     difference-density build in FP32 (a second context whose whole quartet
-    list is on the FP32 path), and a full FP64 build every `full_every`
-    iterations and for the final energy;
+    list is on the FP32 path, with density screening at 1e-12: quartets
+    whose Schwarz bound times the largest difference-density block they
+    touch is below it are skipped) once the density steps are small, a full
+    FP64 build at least every `full_every` iterations, and one for the final
+    energy;
   * the learned-guess hook (guess.py) supplies P0 and the acceptance rule.
 """
 import numpy as np
@@ -96,27 +99,35 @@ def first_energy(H, enuc, P, G):
 
 
 def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8,
-        incremental=None, full_every=8):
+        incremental=None, full_every=8, incremental_below=1e-4):
     """Run RHF to convergence.  engine: FockEngine (its fock_rhf gives
     G = J - K/2).  P0: starting density (default: the core-Hamiltonian
     guess); G0: G(P0) if the caller already built it (the guess hook does).
     incremental: an optional second FockEngine on the same basis set to
     mixed precision with an fp32_bound above every Schwarz bound, used for
-    the difference-density builds.  Returns a dict with energy, iterations,
-    converged, P, C, eps, history and the first-iteration energy."""
+    the difference-density builds once max|P - P_built| < incremental_below
+    (an FP32 build of a large difference would carry ~1e-7 relative errors
+    into every later G until the next full build), with a full build at
+    least every full_every iterations.  Returns a dict with energy,
+    iterations, converged, P, C, eps, history and the first-iteration
+    energy."""
     nb = H.shape[0]
     X = orthogonaliser(S)
     P = hcore_density(H, X, nocc) if P0 is None else np.array(P0, dtype=np.float64)
     max_iter = max_iter or max_cycles(nb)
     diis = Pulay(diis_depth)
-    E_prev, G, P_built, history, E_first = 0.0, None, None, [], None
+    E_prev, G, P_built, history, E_first, since_full = 0.0, None, None, [], None, 0
     for it in range(1, max_iter + 1):
         if it == 1 and G0 is not None:
             G = np.array(G0, dtype=np.float64)
-        elif incremental is not None and G is not None and (it - 1) % full_every:
+            since_full = 0
+        elif (incremental is not None and G is not None and since_full + 1 < full_every
+              and float(np.abs(P - P_built).max()) < incremental_below):
             G = G + incremental.fock_rhf(P - P_built)
+            since_full += 1
         else:
             G = engine.fock_rhf(P)
+            since_full = 0
         P_built = P
         F = H + G
         E = 0.5 * float(np.sum(P * (H + F))) + enuc
@@ -160,6 +171,7 @@ class System:
             from . import FockEngine
             self._incr = FockEngine(self.shells, device=self.device, engine=self.engine.engine, precision="mixed",
                                     fp32_bound=1e300)
+            self._incr.set_density_screening(1e-12)
         return self._incr
 
     def run(self, P0=None, incremental=False, **kw):

