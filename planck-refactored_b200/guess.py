@@ -25,8 +25,8 @@ gets a density built here instead of the default core-Hamiltonian one:
      method, so the guess changes the iteration count, never the answer.
 
 Training data are converged densities of seed-generated alkane conformers
-from the plain GPU SCF (scf.py on the GPU Fock build).  The model is tied to
-one basis set (6-31G* for H and C as trained).
+from the plain GPU SCF (scf.py on the GPU Fock build).  A model is tied to
+the basis set it was trained in (H and C; 6-31G* and cc-pVDZ are shipped).
 """
 import json
 import time
@@ -262,13 +262,20 @@ def purify(P, S, nocc):
 # ---------------------------------------------------------------------------
 # Model
 # ---------------------------------------------------------------------------
+def element_nao(basis_name, library=None):
+    """Cartesian functions per element (H, C) in a basis set."""
+    from .basis import load_library
+    lib = library or load_library()
+    return {e: int(sum((int(L) + 1) * (int(L) + 2) // 2 for L, _ in lib[basis_name][e])) for e in ("H", "C")}
+
+
 class GuessModel:
     """Five networks (one per pair type) and their output standardisation."""
 
     def __init__(self, basis_name="6-31g*", nao=None, device=0, max_batch=8192, seed=0, params=None, stats=None):
         from .mlp import MLP
         self.basis_name, self.device = basis_name, device
-        self.nao = nao or {"C": 15, "H": 2}
+        self.nao = nao or element_nao(basis_name)
         self.out = {"CC": self.nao["C"] ** 2, "CH": self.nao["C"] * self.nao["H"], "HH": self.nao["H"] ** 2,
                     "C": self.nao["C"] ** 2, "H": self.nao["H"] ** 2}
         self.nets, self.stats = {}, stats or {}

@@ -5,7 +5,8 @@
 
 train: seed-generated alkane conformers (C1-C12, linear and branched, bond
 +-0.05 Angstrom, angles +-5 degrees, random torsions; seeds 0..n-1) are
-converged with the plain GPU RHF/6-31G* (scf.py on the GPU Fock build); the
+converged with the plain GPU RHF (6-31G*, or --basis cc-pvdz; scf.py on the
+GPU Fock build); the
 atom-pair features and local-frame density blocks of every converged
 density train the five networks with Adam on the GPU (guess.train).
 
@@ -47,7 +48,7 @@ def conformer(i, lo, hi, seed_base):
     raise RuntimeError(f"no conformer for C{nc}")
 
 
-def generate(n, device=0, log=print):
+def generate(n, device=0, log=print, basis="6-31g*"):
     P = _pkg()
     G = P.guess
     lib = P.basis.load_library()
@@ -55,7 +56,7 @@ def generate(n, device=0, log=print):
     iters, t0 = [], time.perf_counter()
     for i in range(n):
         nc, atoms = conformer(i, 1, 12, 0)
-        sysm = P.scf.System(atoms, "6-31g*", lib, device=device)
+        sysm = P.scf.System(atoms, basis, lib, device=device)
         r = sysm.run()
         if not r["converged"]:
             sysm.close()
@@ -77,9 +78,9 @@ def generate(n, device=0, log=print):
 def cmd_train(args):
     P = _pkg()
     G = P.guess
-    samples, info = generate(args.n, args.device)
+    samples, info = generate(args.n, args.device, basis=args.basis)
     print(json.dumps({"data": info}), flush=True)
-    model = G.GuessModel("6-31g*", device=args.device, seed=args.seed)
+    model = G.GuessModel(args.basis, device=args.device, seed=args.seed)
     t0 = time.perf_counter()
     losses = G.train(model, samples, epochs=args.epochs, lr=args.lr, batch=args.batch, seed=args.seed,
                      log=(lambda s: print(s, flush=True)) if args.verbose else None)
@@ -92,10 +93,11 @@ def evaluate(model_path, n, device=0, lo=8, hi=20, log=None):
     G = P.guess
     lib = P.basis.load_library()
     model = G.GuessModel.load(model_path, device=device)
+    basis = model.basis_name
     rows = []
     for i in range(n):
         nc, atoms = conformer(i, lo, hi, 1_000_000)
-        sysm = P.scf.System(atoms, "6-31g*", lib, device=device)
+        sysm = P.scf.System(atoms, basis, lib, device=device)
         t0 = time.perf_counter()
         r_d = sysm.run()
         t_d = time.perf_counter() - t0
@@ -115,7 +117,7 @@ def evaluate(model_path, n, device=0, lo=8, hi=20, log=None):
     model.close()
     it_d = np.array([r["it_default"] for r in rows])
     it_l = np.array([r["it_learned"] for r in rows])
-    return {"molecules": n, "basis": "6-31g*", "sizes": f"C{lo}-C{hi}",
+    return {"molecules": n, "basis": basis, "sizes": f"C{lo}-C{hi}",
             "mean_iterations_default": float(it_d.mean()), "mean_iterations_learned": float(it_l.mean()),
             "iterations_ratio": float(it_l.sum() / it_d.sum()),
             "fock_builds_ratio": float(sum(r["builds_learned"] for r in rows) / sum(r["builds_default"] for r in rows)),
@@ -138,6 +140,7 @@ def main():
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--n", type=int, default=4096)
+    t.add_argument("--basis", default="6-31g*", choices=["6-31g*", "cc-pvdz"])
     t.add_argument("--model", default=os.path.join(HERE, "data", "guess_model_631gs.npz"))
     t.add_argument("--epochs", type=int, default=40)
     t.add_argument("--lr", type=float, default=1e-3)
