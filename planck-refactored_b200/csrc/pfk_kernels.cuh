@@ -91,8 +91,12 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
 //   K(i,k) += sum_jl v Pk(j,l)    K(j,k) += sum_il v Pk(i,l)
 //   K(i,l) += sum_jk v Pk(j,k)    K(j,l) += sum_ik v Pk(i,k)
 // (J = 2 (Jacc + Jacc^T) and K = Kacc + Kacc^T afterwards.)
+// warp_bra: every lane of the (full) warp digests a quartet with this same
+// bra block, so the J(i,j) sums are first added across the warp and one lane
+// issues each atomic instead of 32 lanes hitting the same address.
 template <int NA, int NB, int NC, int ND, int NK, typename V>
-__device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args)
+__device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args,
+                                              bool warp_bra = false)
 {
     const int nb = args.nb;
 #define PFK_V(ia, ib, ic, id) double(v[(((ia) * NB + (ib)) * NC + (ic)) * ND + (id)])
@@ -111,7 +115,13 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                 for (int ic = 0; ic < NC; ++ic)
 #pragma unroll
                     for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ic * ND + id];
-                atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+                if (warp_bra) {
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                    if ((threadIdx.x & 31) == 0) atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+                } else {
+                    atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+                }
             }
     }
     asm volatile("" ::: "memory");
@@ -265,7 +275,10 @@ __device__ __forceinline__ void finish_block(R *acc, const uint2 qd, const PairI
                                                      args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
                     acc[c] = acc[c] * R(sw * S::norm(ia, ib, ic, id));
                 }
-    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args);
+    // lanes of a full warp usually share the bra pair (lists are bra-major)
+    const unsigned act = __activemask();
+    const bool warp_bra = act == 0xffffffffu && __all_sync(act, __shfl_sync(act, qd.x, 0) == qd.x);
+    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args, warp_bra);
 }
 
 // ---------------------------------------------------------------------------

@@ -349,15 +349,13 @@ __global__ void __launch_bounds__(128) eri_os_kernel(const uint2 *__restrict__ q
 #pragma unroll
     for (int c = 0; c < O::NACC; ++c) acc[c] = R(0);
     // Primitive loops, ket outer (the lanes of a warp mostly share the bra
-    // pair, so bra loads are broadcasts).  The next bra primitive's load is
-    // issued before the current one is evaluated, so its latency overlaps the
-    // Boys function and the recurrence instead of stalling the loop.
+    // pair, so bra loads are broadcasts).  Loading the next bra primitive
+    // ahead of the current one was measured slower: its registers cost more
+    // occupancy than the latency it hides.
     for (int jp = 0; jp < pk.nprim; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
-        PrimPair pn = load_prim(args.prims, pb.prim_off);
         for (int ip = 0; ip < pb.nprim; ++ip) {
-            const PrimPair p = pn;
-            if (ip + 1 < pb.nprim) pn = load_prim(args.prims, pb.prim_off + ip + 1);
+            const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
             if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
             const QuartetScalars s = quartet_scalars(p, q);
             double Fm[L + 1];
