@@ -67,7 +67,8 @@ static __constant__ const BoysSeriesTable kBoysSeries = make_boys_series_table()
 
 // Boys function F_m(T), m = 0..M (M <= 6).  T below TS: the Taylor series of
 // F_M and downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1), which is
-// stable.  T >= TS: F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T and the upward
+// stable.  T >= TS: F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T (with erf(sqrt T) =
+// 1 - e^-T erfcx(sqrt T), so one exponential serves all m) and the upward
 // recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T); its error growth stays
 // below ~10x for m <= 4 at T >= 2 (~2x for m <= 1 at T >= 1; TS = 3 for
 // m = 5, 6).  T >= TA (50, or 60 for M > 4): the large-T limit F_0 =
@@ -91,10 +92,12 @@ __device__ __forceinline__ void boys_fm(double T, double *F)
             for (int m = M - 1; m >= 0; --m) F[m] = fma(2.0 * T, F[m + 1], e) * (1.0 / (2 * m + 1));
         }
     } else if (T < TA) {
+        // erf(sqrt T) = 1 - e^-T erfcx(sqrt T): one exponential serves both
+        // F_0 and the recursion (erfc(sqrt T) <= erfc(1) = 0.16, no cancellation)
         const double ist = rsqrt(T);
-        F[0] = 0.88622692545275801365 * erf(T * ist) * ist;   // sqrt(pi)/2
+        const double e = exp(-T);
+        F[0] = 0.88622692545275801365 * fma(-e, erfcx(T * ist), 1.0) * ist;   // sqrt(pi)/2
         if constexpr (M > 0) {
-            const double e = exp(-T);
             const double h = 0.5 * ist * ist;                     // 1/(2T)
 #pragma unroll
             for (int m = 0; m < M; ++m) F[m + 1] = fma(double(2 * m + 1), F[m], -e) * h;

@@ -4,18 +4,20 @@ boys_fm<M> in csrc/pfk_os.cuh evaluates F_0..F_M (M <= 6) as follows:
   * T below TS (1 for M <= 1, 2 for M <= 4, 3 above): the Taylor series of
     F_M, sum_k (-T)^k / (k! (2M+2k+1)), with 18, 25 or 32 terms, then the
     downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1);
-  * up to TA (50 for M <= 4, 60 above) F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T
-    and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T);
+  * up to TA (50 for M <= 4, 60 above) F_0 = sqrt(pi)/2 erf(sqrt T)/sqrt T,
+    with erf(sqrt T) = 1 - e^-T erfcx(sqrt T), and the upward recursion
+    F_{m+1} = ((2m+1) F_m - e^-T) / (2T);
   * above TA the large-T limit F_0 = sqrt(pi/4T), F_{m+1} = (2m+1) F_m / (2T).
-This test restates that scheme in double precision with the C library's erf
-and exp and checks it against 40-digit Boys values.  The scheme's parameters
-(thresholds, term counts) are what the device code uses.  The device's erf
+This test restates that scheme in double precision with the C library's exp
+and scipy's erfcx and checks it against 40-digit Boys values.  The scheme's parameters
+(thresholds, term counts) are what the device code uses.  The device's erfcx
 and exp differ from the C library's by a few ulp, which the GPU integral tests
 cover."""
 import math
 
 import numpy as np
 import pytest
+from scipy.special import erfcx
 
 mpmath = pytest.importorskip("mpmath")
 
@@ -37,8 +39,8 @@ def boys_scheme(M, T):
             F[m] = (2.0 * T * F[m + 1] + e) * (1.0 / (2 * m + 1))
     elif T < (50.0 if M <= 4 else 60.0):
         ist = 1.0 / math.sqrt(T)
-        F[0] = 0.88622692545275801365 * math.erf(T * ist) * ist
         e = math.exp(-T)
+        F[0] = 0.88622692545275801365 * (1.0 - e * erfcx(T * ist)) * ist
         h = 0.5 * ist * ist
         for m in range(M):
             F[m + 1] = ((2 * m + 1) * F[m] - e) * h
