@@ -94,13 +94,14 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
 // warp_bra: every lane of the (full) warp digests a quartet with this same
 // bra block, so the J(i,j) sums are first added across the warp and one lane
 // issues each atomic instead of 32 lanes hitting the same address.
-template <int NA, int NB, int NC, int ND, int NK, typename V>
+// SKIP_JIJ: the caller has already added the J(i,j) block.
+template <int NA, int NB, int NC, int ND, int NK, bool SKIP_JIJ = false, typename V>
 __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args,
                                               bool warp_bra = false)
 {
     const int nb = args.nb;
 #define PFK_V(ia, ib, ic, id) double(v[(((ia) * NB + (ib)) * NC + (ic)) * ND + (id)])
-    {
+    if constexpr (!SKIP_JIJ) {
         double p[NC * ND];
 #pragma unroll
         for (int ic = 0; ic < NC; ++ic)
@@ -684,10 +685,9 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
             split_sync<TEAM>(mask, team);
         }
     }
-    if (!owner) return;
-
     // ---- digestion of this thread's components: A index ia, B indices
-    // ib0 .. ib0 + NBT - 1, all C and D ----
+    // ib0 .. ib0 + NBT - 1, all C and D.  Non-owner lanes hold a zero block
+    // (ia = 0) and take part only in the J(i,j) reduction across teams. ----
     const int nb = args.nb;
     const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
     const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
@@ -695,6 +695,7 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
     const int i = i0 + ia;
 
     if (args.eri_out) {
+        if (!owner) return;
 #pragma unroll
         for (int bl = 0; bl < NBT; ++bl)
 #pragma unroll
@@ -724,7 +725,36 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                 acc[(bl * NC + ic) * ND + id] *=
                     sw * cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
             }
-    digest_blocks<1, NBT, NC, ND, NK>(acc, i, j0 + ib0, k0, l0, args);
+    // J(i, j0+ib0+bl): the teams of a warp usually share the bra pair, and a
+    // lane's (ia, ib0) depends only on its place in the team, so lanes TEAM
+    // apart add their sums before one team's owners issue the atomics.
+    {
+        const unsigned act = __activemask();
+        const bool warp_bra = TEAM < 32 && act == 0xffffffffu &&
+                              __all_sync(act, __shfl_sync(act, qd.x, 0) == qd.x);
+        double p[NC * ND];
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+            for (int id = 0; id < ND; ++id) p[ic * ND + id] = __ldg(args.Pj + (size_t)(k0 + ic) * nb + l0 + id);
+#pragma unroll
+        for (int bl = 0; bl < NBT; ++bl) {
+            double sj = 0.0;
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) sj += acc[(bl * NC + ic) * ND + id] * p[ic * ND + id];
+            if (warp_bra) {
+#pragma unroll
+                for (int o = TEAM; o < 32; o <<= 1) sj += __shfl_xor_sync(0xffffffffu, sj, o);
+                if (owner && (threadIdx.x & 31) < TEAM) atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, sj);
+            } else if (owner) {
+                atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, sj);
+            }
+        }
+    }
+    if (!owner) return;
+    digest_blocks<1, NBT, NC, ND, NK, true>(acc, i, j0 + ib0, k0, l0, args);
 }
 
 }  // namespace pfk
