@@ -2,7 +2,7 @@
 functions) on B200, one process per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed]
+                    [--precision fp64|mixed] [--engine auto|os|rys]
 
 A step is one Fock build G = J(P) - K(P)/2 of (H2O)32 / 6-31G** (Cartesian,
 800 functions), tol_eri 1e-10, on a seeded symmetric density (the build's work
@@ -10,7 +10,10 @@ does not depend on the density values).  By default the build is the mixed-
 precision one of the benchmark configuration (FP32 arithmetic for quartets
 whose Schwarz bound is below 1e-8, FP64 roots, weights and accumulation); the
 all-FP64 build is timed beside it and its speed-up and G / energy error are
-reported.  With N > 1 (torchrun, NCCL) every rank evaluates every N-th
+reported.  The engine is `auto`: the per-class kernel choice (Rys, Obara-
+Saika, or Obara-Saika at higher occupancy) is measured by the library's
+autotuner on this molecule's lists during setup.  With N > 1 (torchrun, NCCL)
+every rank evaluates every N-th
 quartet of each class's screened quartet list and the partial G are summed
 with one all-reduce per build:
 strong scaling of one build.
@@ -207,6 +210,11 @@ def ours_arm(args):
     t0 = time.perf_counter()
     eng = P.FockEngine(shells, device=local, engine=args.engine, precision=args.precision, fp32_bound=1e-8)
     t_setup = time.perf_counter() - t0
+    tuned, t_tune = None, 0.0
+    if args.engine == "auto":   # per-class kernel choice measured on this molecule's lists
+        t0 = time.perf_counter()
+        tuned = eng.autotune()
+        t_tune = time.perf_counter() - t0
     if world > 1:
         eng.set_shard(rank, world)
     nb = eng.nbasis
@@ -303,6 +311,8 @@ def ours_arm(args):
         torch.cuda.synchronize()
         G_mixed = dG.cpu().numpy().copy()
         e64 = P.FockEngine(shells, device=local, engine=args.engine, precision="fp64")
+        if args.engine == "auto":
+            e64.autotune()
         if world > 1:
             e64.set_shard(rank, world)
         ms64 = device_ms(e64, max(3, args.steps // 2))
@@ -363,6 +373,9 @@ def ours_arm(args):
                 "classes_ms": {k: round(v[2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "classes_primitive_quartets": {k: v[1] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "classes_shell_quartets": {k: v[0] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
+                "autotune": None if tuned is None else
+                {"seconds": t_tune, "choice": {k: v[0] for k, v in tuned.items()
+                                               if k in dict(sorted(cls.items(), key=lambda kv: -kv[1][2])[:12])}},
                 "classes_ms_rys_kernels": None if cls_rys is None else
                 {k: round(cls_rys[k][2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "clocks": clk}
@@ -386,8 +399,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--engine", choices=["os", "rys", "auto"], default="os",
-                    help="integral engine (the reference's option; os is its default)")
+    ap.add_argument("--engine", choices=["os", "rys", "auto"], default="auto",
+                    help="integral engine (the reference's option); auto runs the autotuner at setup")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="mixed: FP32 below a Schwarz bound of 1e-8 (the benchmark configuration); "
                          "the all-FP64 build is timed beside it")

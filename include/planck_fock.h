@@ -151,6 +151,19 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
  * reference's); dtol = 0 turns it off.  Not in the reference. */
 pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol);
 
+/* Autotuner for engine auto: times every candidate kernel of every class on
+ * this context's screened lists (a warm-up pass, then the faster of two timed
+ * passes) and keeps the fastest per class for the builds made with engine
+ * auto.  Candidates: 0 = Rys, 2 = Obara-Saika, 6 = Obara-Saika compiled for 4
+ * blocks of 128 threads per SM; the last two exist for classes with
+ * LA+LB+LC+LD <= 4, the others always run Rys.  Until it runs, engine auto
+ * uses the reference's outcome (OS for L <= 4, Rys above).  choice55 (may be
+ * NULL) receives the chosen candidate per class, ms55x3 (may be NULL) the
+ * measured milliseconds per class and candidate (0 when not applicable).
+ * The reference chooses per component quartet from a cost model
+ * (rys.cpp:195-236); this chooses per class from measurements. */
+pfk_status pfk_autotune(pfk_ctx *ctx, int *choice55, double *ms55x3);
+
 /* Measurement helper: sustained FP64 and FP32 fused-multiply-add throughput
  * of `device` in TFLOP/s (2 flops per FMA), from a register-resident FMA
  * loop over all SMs, timed with CUDA events.  The FP64 figure is the

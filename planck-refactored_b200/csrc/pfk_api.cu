@@ -94,6 +94,9 @@ struct pfk_ctx {
     long long q32_off[kQuartetClasses] = {}, q32_cnt[kQuartetClasses] = {};
     ClassLauncher launch[kQuartetClasses] = {};
     float class_ms[kQuartetClasses] = {};
+    // engine auto: launch flags per class (kLaunchOS / kLaunchDense or 0 for
+    // Rys); the static rule until pfk_autotune measures the candidates
+    int auto_flags[kQuartetClasses] = {};
 
     DevBuf<double> d_P, d_Pb, d_Pt, d_J, d_K0, d_K1, d_G, d_Gb;
     std::vector<GraphEntry> graphs;
@@ -396,6 +399,18 @@ pfk_status schwarz_and_sort(pfk_ctx *ctx)
     return PFK_OK;
 }
 
+// Kernel choice of class c.  engine os: the Obara-Saika kernel for the
+// classes that have one (L <= kOSMaxL, where the reference's per-quartet auto
+// choice is OS for every component quartet), Rys for the rest; engine rys:
+// Rys; engine auto: the per-class choice of pfk_autotune (the os rule until
+// it has run).
+int class_flags(const pfk_ctx *ctx, int c)
+{
+    if (ctx->engine == PFK_ENGINE_RYS) return 0;
+    if (ctx->engine == PFK_ENGINE_AUTO) return ctx->auto_flags[c];
+    return quartet_class_L(c) <= kOSMaxL ? kLaunchOS : 0;
+}
+
 // Launch every class kernel over the screened lists.  Jacc/K accumulators are
 // zeroed first.  eri_out selects the dense-tensor mode.
 pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const double *Pk1, int nk, double *Jacc,
@@ -440,10 +455,7 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         const long long nh = local(ctx->q_cnt[c]), nl = local(ctx->q32_cnt[c]);
         if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
-        // engine os / auto: Obara-Saika kernels for the classes that have them
-        // (L <= kOSMaxL, where the reference's per-quartet auto choice is OS
-        // for every component quartet), Rys for the rest; engine rys: Rys.
-        const int os = (ctx->engine != PFK_ENGINE_RYS && quartet_class_L(c) <= kOSMaxL) ? kLaunchOS : 0;
+        const int os = class_flags(ctx, c);
         const int fp32 = ctx->precision == PFK_PREC_MIXED ? kLaunchFP32 : 0;
         if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, os, st);
         if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, os | fp32, st);
@@ -562,6 +574,7 @@ pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
                 return bail(PFK_ERR_STATE);
             }
             ctx->launch[c] = g_class_launchers[c];
+            ctx->auto_flags[c] = quartet_class_L(c) <= kOSMaxL ? kLaunchOS : 0;
         }
         JKArgs none{};
         for (int c = 0; c < kQuartetClasses; ++c) ctx->launch[c](nullptr, -1, none, 1, 0, ctx->stream);
@@ -824,6 +837,52 @@ pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_
         if (prim_quartets55) prim_quartets55[c] = ctx->prim_cnt[c];
     }
     return PFK_OK;
+}
+
+pfk_status pfk_autotune(pfk_ctx *ctx, int *choice55, double *ms55x3)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    pfk_status s = ensure_work(ctx);
+    if (s != PFK_OK) return s;
+    const size_t nb2 = (size_t)ctx->nb * ctx->nb;
+    PFK_CK(cudaMemsetAsync(ctx->d_P.p, 0, sizeof(double) * nb2, ctx->stream));   // timing only needs a density
+    // candidates: Rys, Obara-Saika, Obara-Saika at 4 blocks/SM (L <= kOSMaxL only)
+    const int candidates[3] = {0, kLaunchOS, kLaunchOS | kLaunchDense};
+    double t[kQuartetClasses][3] = {};
+    const int engine = ctx->engine;
+    int chosen[kQuartetClasses];
+    for (int c = 0; c < kQuartetClasses; ++c) chosen[c] = ctx->auto_flags[c];
+    ctx->engine = PFK_ENGINE_AUTO;
+    for (int v = 0; v < 3 && s == PFK_OK; ++v) {
+        for (int c = 0; c < kQuartetClasses; ++c)
+            ctx->auto_flags[c] = quartet_class_L(c) <= kOSMaxL ? candidates[v] : 0;
+        for (int rep = 0; rep < 3 && s == PFK_OK; ++rep) {   // a warm-up pass, then the faster of two
+            s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, ctx->d_K0.p, nullptr, nullptr,
+                            ctx->stream, true);
+            if (rep == 0) continue;
+            for (int c = 0; c < kQuartetClasses; ++c)
+                if (t[c][v] == 0.0 || ctx->class_ms[c] < t[c][v]) t[c][v] = ctx->class_ms[c];
+        }
+    }
+    for (int c = 0; c < kQuartetClasses && s == PFK_OK; ++c) {
+        if (ctx->q_cnt[c] + ctx->q32_cnt[c] == 0) continue;
+        const int nv = quartet_class_L(c) <= kOSMaxL ? 3 : 1;
+        int best = 0;
+        for (int v = 1; v < nv; ++v)
+            if (t[c][v] < t[c][best]) best = v;
+        chosen[c] = candidates[best];
+    }
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        ctx->auto_flags[c] = chosen[c];
+        if (choice55) choice55[c] = chosen[c];
+        if (ms55x3)
+            for (int v = 0; v < 3; ++v)
+                ms55x3[3 * c + v] = (v == 0 || quartet_class_L(c) <= kOSMaxL) ? t[c][v] : 0.0;
+    }
+    ctx->engine = engine;
+    drop_graphs(ctx);   // captured builds hold the old choices
+    return s;
 }
 
 pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol)

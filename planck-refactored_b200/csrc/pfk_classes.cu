@@ -25,8 +25,11 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int flag
         if (flags & kLaunchOS) {
             if (n <= 0) return;
             const long long grid = (n + 127) / 128;
+            const bool dense = flags & kLaunchDense;
             if (nk == 2) eri_os_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else if (fp32 && dense) eri_os_kernel<LA, LB, LC, LD, 1, float, 4><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             else if (fp32) eri_os_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else if (dense) eri_os_kernel<LA, LB, LC, LD, 1, double, 4><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             else eri_os_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             return;
         }

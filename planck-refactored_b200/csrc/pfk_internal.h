@@ -29,7 +29,9 @@ __host__ __device__ constexpr int quartet_class_L(int c)
 // class has one (register-path and Obara-Saika classes with nk == 1; the
 // others run FP64).  kLaunchOS asks for the Obara-Saika kernel, which exists
 // for classes with LA+LB+LC+LD <= kOSMaxL; the other classes run Rys.
-constexpr int kLaunchFP32 = 1, kLaunchOS = 2;
+// kLaunchDense picks the Obara-Saika kernel compiled for 4 blocks of 128
+// per SM (single exchange density only).
+constexpr int kLaunchFP32 = 1, kLaunchOS = 2, kLaunchDense = 4;
 constexpr int kOSMaxL = 4;
 
 // One launcher per quartet class.  nk = number of exchange densities (1 or 2).

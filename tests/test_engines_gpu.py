@@ -96,3 +96,31 @@ def test_uhf_and_mixed_precision_on_os_kernels():
     eng.close()
     assert np.abs(Gmx - G64).max() < 1e-7
     assert abs(0.5 * np.sum(Pa * (Gmx - G64))) < 1e-6
+
+
+def test_autotune_picks_per_class_and_keeps_results(random_basis):
+    """pfk_autotune times every candidate per class and keeps the fastest for
+    engine auto: classes above L = 4 can only run Rys, the builds before and
+    after agree to rounding, and switching engine and back keeps the choice."""
+    P = pfk()
+    eng = P.FockEngine(random_basis, engine="auto")
+    nb = eng.nbasis
+    Pm = random_density(nb, seed=12)
+    G0 = eng.fock_rhf(Pm)
+    res = eng.autotune()
+    assert res
+    for name, (choice, times) in res.items():
+        L = sum("spdf".index(ch) for ch in name if ch in "spdf")
+        assert choice in ("rys", "os", "os-dense")
+        if L > 4:
+            assert choice == "rys" and set(times) == {"rys"}
+        else:
+            assert set(times) == {"rys", "os", "os-dense"}
+            assert times[choice] == min(times.values())
+    G1 = eng.fock_rhf(Pm)
+    eng.set_options(1e-10, "rys")
+    eng.set_options(1e-10, "auto")
+    G2 = eng.fock_rhf(Pm)
+    eng.close()
+    assert np.abs(G1 - G0).max() < 1e-11
+    assert np.abs(G2 - G1).max() < 1e-13
