@@ -94,14 +94,16 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
 // warp_bra: every lane of the (full) warp digests a quartet with this same
 // bra block, so the J(i,j) sums are first added across the warp and one lane
 // issues each atomic instead of 32 lanes hitting the same address.
-// SKIP_JIJ: the caller has already added the J(i,j) block.
-template <int NA, int NB, int NC, int ND, int NK, bool SKIP_JIJ = false, typename V>
+// SKIP: blocks the caller has already added (kSkipJij, kSkipJkl, kSkipKjk,
+// kSkipKjl bits).
+constexpr int kSkipJij = 1, kSkipJkl = 2, kSkipKjk = 4, kSkipKjl = 8;
+template <int NA, int NB, int NC, int ND, int NK, int SKIP = 0, typename V>
 __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args,
                                               bool warp_bra = false)
 {
     const int nb = args.nb;
 #define PFK_V(ia, ib, ic, id) double(v[(((ia) * NB + (ib)) * NC + (ic)) * ND + (id)])
-    if constexpr (!SKIP_JIJ) {
+    if constexpr (!(SKIP & kSkipJij)) {
         double p[NC * ND];
 #pragma unroll
         for (int ic = 0; ic < NC; ++ic)
@@ -126,7 +128,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
             }
     }
     asm volatile("" ::: "memory");
-    {
+    if constexpr (!(SKIP & kSkipJkl)) {
         double p[NA * NB];
 #pragma unroll
         for (int ia = 0; ia < NA; ++ia)
@@ -169,7 +171,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                 }
         }
         asm volatile("" ::: "memory");
-        {   // K(j,k) from Pk(i,l)
+        if constexpr (!(SKIP & kSkipKjk)) {   // K(j,k) from Pk(i,l)
             double p[NA * ND];
 #pragma unroll
             for (int ia = 0; ia < NA; ++ia)
@@ -207,7 +209,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                 }
         }
         asm volatile("" ::: "memory");
-        {   // K(j,l) from Pk(i,k)
+        if constexpr (!(SKIP & kSkipKjl)) {   // K(j,l) from Pk(i,k)
             double p[NA * NC];
 #pragma unroll
             for (int ia = 0; ia < NA; ++ia)
@@ -561,6 +563,13 @@ struct SplitShape {
     static constexpr int NIP = (LA + 1) * AST;                 // padded table per (root, axis)
     static constexpr int TABLE = S::NR * 3 * NIP + (S::NR * 3 * NIP + 1) % 2;
     static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
+    // team reduction of the blocks every owner adds to the same elements of
+    // (LEVEL 1: J(k,l), K(j,k), K(j,l)), staged in the team's table after the
+    // primitive loop: REDV partial sums per owner per exchange density
+    static constexpr int REDV1 = S::NC * S::ND, REDVK = S::NB * S::NC + S::NB * S::ND;
+    template <int NK>
+    __host__ __device__ static constexpr int redv() { return REDV1 + NK * REDVK; }
+    static constexpr bool TEAMRED = LEVEL == 1 && TEAM <= 32 && (REDV1 + 2 * REDVK) * GROUP <= TABLE;
     static constexpr bool OK = TEAM <= 128 && M <= 64;
 };
 
@@ -753,8 +762,75 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
             }
         }
     }
+    if constexpr (SS::TEAMRED) {
+        // owners stage their partial sums of J(k,l), K_m(j,k), K_m(j,l) in the
+        // team's (now unused) table; the team then adds them up and one lane
+        // per element issues the atomic
+        constexpr int V = SS::template redv<NK>();
+        double *red = g;
+        split_sync<TEAM>(mask, team);
+        if (owner) {
+            {
+                double pij[NB];
+#pragma unroll
+                for (int bl = 0; bl < NB; ++bl) pij[bl] = __ldg(args.Pj + (size_t)i * nb + j0 + bl);
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) {
+                        double sj = 0.0;
+#pragma unroll
+                        for (int bl = 0; bl < NB; ++bl) sj += acc[(bl * NC + ic) * ND + id] * pij[bl];
+                        red[gi * V + ic * ND + id] = sj;
+                    }
+            }
+#pragma unroll
+            for (int m = 0; m < NK; ++m) {
+                const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
+                double *r = red + gi * V + SS::REDV1 + m * SS::REDVK;
+                if (!(m == 0 ? args.Kacc0 : args.Kacc1)) continue;
+                double pil[ND], pik[NC];
+#pragma unroll
+                for (int id = 0; id < ND; ++id) pil[id] = __ldg(Pk + (size_t)i * nb + l0 + id);
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic) pik[ic] = __ldg(Pk + (size_t)i * nb + k0 + ic);
+#pragma unroll
+                for (int bl = 0; bl < NB; ++bl) {
+#pragma unroll
+                    for (int ic = 0; ic < NC; ++ic) {
+                        double sk = 0.0;
+#pragma unroll
+                        for (int id = 0; id < ND; ++id) sk += acc[(bl * NC + ic) * ND + id] * pil[id];
+                        r[bl * NC + ic] = sk;                              // K(j,k)
+                    }
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) {
+                        double sk = 0.0;
+#pragma unroll
+                        for (int ic = 0; ic < NC; ++ic) sk += acc[(bl * NC + ic) * ND + id] * pik[ic];
+                        r[NB * NC + bl * ND + id] = sk;                    // K(j,l)
+                    }
+                }
+            }
+        }
+        split_sync<TEAM>(mask, team);
+        for (int e = lane; e < V; e += TEAM) {
+            double sum = 0.0;
+            for (int o = 0; o < SS::GROUP; ++o) sum += red[o * V + e];
+            if (e < SS::REDV1) {
+                atomicAdd(args.Jacc + (size_t)(k0 + e / ND) * nb + l0 + e % ND, sum);
+            } else {
+                const int m = (e - SS::REDV1) / SS::REDVK, f = (e - SS::REDV1) % SS::REDVK;
+                double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+                if (!Kacc) continue;
+                if (f < NB * NC) atomicAdd(Kacc + (size_t)(j0 + f / NC) * nb + k0 + f % NC, sum);
+                else atomicAdd(Kacc + (size_t)(j0 + (f - NB * NC) / ND) * nb + l0 + (f - NB * NC) % ND, sum);
+            }
+        }
+    }
     if (!owner) return;
-    digest_blocks<1, NBT, NC, ND, NK, true>(acc, i, j0 + ib0, k0, l0, args);
+    digest_blocks<1, NBT, NC, ND, NK, kSkipJij | (SS::TEAMRED ? kSkipJkl | kSkipKjk | kSkipKjl : 0)>(
+        acc, i, j0 + ib0, k0, l0, args);
 }
 
 }  // namespace pfk
