@@ -215,6 +215,7 @@ def ours_arm(args):
         t0 = time.perf_counter()
         tuned = eng.autotune()
         t_tune = time.perf_counter() - t0
+    eng.set_lanes(args.lanes)
     if world > 1:
         eng.set_shard(rank, world)
     nb = eng.nbasis
@@ -313,6 +314,7 @@ def ours_arm(args):
         e64 = P.FockEngine(shells, device=local, engine=args.engine, precision="fp64")
         if args.engine == "auto":
             e64.autotune()
+        e64.set_lanes(args.lanes)
         if world > 1:
             e64.set_shard(rank, world)
         ms64 = device_ms(e64, max(3, args.steps // 2))
@@ -351,6 +353,7 @@ def ours_arm(args):
                 "data": "synthetic (seeded water cluster, Basis Set Exchange 6-31G**)",
                 "config": {"workload": WORKLOAD if args.waters == 32 else f"(H2O){args.waters} 6-31G** ({nb} bf)",
                            "nbasis": nb, "tol_eri": 1e-10, "precision": args.precision, "engine": args.engine,
+                           "lanes": args.lanes,
                            "parallelism": f"quartet-list shards x{world} + NCCL all-reduce of G" if world > 1
                            else "single GPU", "l2": "inputs larger than L2: the screened quartet lists "
                            f"({n_shell * 8 / 1e9:.2f} GB) and primitive-pair data stream from HBM every build",
@@ -407,6 +410,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU sampling for cpu_baseline")
     ap.add_argument("--ref-budget", type=float, default=8.0, help="seconds of CPU sampling per reference step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 3, 4],
+                    help="streams the class kernels of a build are spread over")
     ap.add_argument("--waters", type=int, default=32,
                     help="cluster size; 32 is the benchmark workload, smaller sizes are for profiling")
     args = ap.parse_args()

@@ -151,6 +151,16 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks);
  * reference's); dtol = 0 turns it off.  Not in the reference. */
 pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol);
 
+/* Concurrent class launches: every later build of this context issues its
+ * class kernels on `lanes` streams (1 to 4; default 4) forked from the
+ * build's stream and joined back before the J/K combine, so that one class's
+ * tail and the small classes overlap the others.  Classes go, largest
+ * (primitive quartets x component quartets) first, to the lane with the
+ * least work.  lanes = 1 issues them in class order on the build's stream.
+ * The results differ only by the order of the FP64 atomic additions.
+ * Not in the reference (its loop over quartets is one OpenMP region). */
+pfk_status pfk_set_lanes(pfk_ctx *ctx, int lanes);
+
 /* Autotuner for engine auto: times every candidate kernel of every class on
  * this context's screened lists (a warm-up pass, then the faster of two timed
  * passes) and keeps the fastest per class for the builds made with engine

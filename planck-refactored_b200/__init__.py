@@ -30,7 +30,7 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
            "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
-           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
+           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step"]
 
@@ -80,6 +80,7 @@ def load_library(path=LIB_PATH):
     L.pfk_fock_rhf_noalloc.argtypes = [ctypes.POINTER(BasisDesc), vp, vp, c_dbl, vp]
     L.pfk_one_electron.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, vp, vp, vp, c_int]
     L.pfk_set_density_screening.argtypes = [vp, c_dbl]
+    L.pfk_set_lanes.argtypes = [vp, c_int]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
     return L
@@ -218,6 +219,10 @@ class FockEngine:
             if t:
                 out[CLASS_NAMES[c]] = (names[int(choice[c])], t)
         return out
+
+    def set_lanes(self, lanes):
+        """Streams the class kernels of a build are spread over (1 to 4)."""
+        self._check(self.lib.pfk_set_lanes(self.h, int(lanes)))
 
     def set_density_screening(self, dtol):
         """Skip shell quartets whose Schwarz bound times the largest density

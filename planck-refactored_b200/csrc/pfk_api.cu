@@ -56,10 +56,17 @@ struct GraphEntry {
 
 }  // namespace
 
+constexpr int kMaxLanes = 4;
+
 struct pfk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    // concurrent class launches: lanes - 1 side streams forked from the
+    // build's stream (fork_ev) and joined back (join_ev) around the classes
+    int lanes = kMaxLanes;
+    cudaStream_t side[kMaxLanes - 1] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes - 1] = {};
 
     int nshell = 0, nb = 0;
     std::vector<int> L, bf_off;
@@ -411,6 +418,15 @@ int class_flags(const pfk_ctx *ctx, int c)
     return quartet_class_L(c) <= kOSMaxL ? kLaunchOS : 0;
 }
 
+// Cartesian component quartets of class c (the launch-order cost weight).
+static int class_components(int c)
+{
+    int x = 0;
+    while ((x + 1) * (x + 2) / 2 <= c) ++x;
+    const int y = c - x * (x + 1) / 2;
+    return ncart(pc_la(x)) * ncart(pc_lb(x)) * ncart(pc_la(y)) * ncart(pc_lb(y));
+}
+
 // Launch every class kernel over the screened lists.  Jacc/K accumulators are
 // zeroed first.  eri_out selects the dense-tensor mode.
 pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const double *Pk1, int nk, double *Jacc,
@@ -451,14 +467,39 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
         PFK_CK(cudaEventCreate(&ev[0]));
         PFK_CK(cudaEventCreate(&ev[1]));
     }
+    // lanes: the classes go, largest estimated cost first, to the lane with
+    // the least work so far; a per-class timed pass stays on one stream
+    const int nlanes = timed ? 1 : ctx->lanes;
+    cudaStream_t lane_st[kMaxLanes] = {st};
+    if (nlanes > 1) {
+        PFK_CK(cudaEventRecord(ctx->fork_ev, st));
+        for (int i = 1; i < nlanes; ++i) {
+            lane_st[i] = ctx->side[i - 1];
+            PFK_CK(cudaStreamWaitEvent(lane_st[i], ctx->fork_ev, 0));
+        }
+    }
+    int order[kQuartetClasses];
+    double cost[kQuartetClasses];
     for (int c = 0; c < kQuartetClasses; ++c) {
+        order[c] = c;
+        cost[c] = (double)ctx->prim_cnt[c] * class_components(c);
+    }
+    if (nlanes > 1)
+        std::stable_sort(order, order + kQuartetClasses, [&](int x, int y) { return cost[x] > cost[y]; });
+    double load[kMaxLanes] = {};
+    for (int oc = 0; oc < kQuartetClasses; ++oc) {
+        const int c = order[oc];
         const long long nh = local(ctx->q_cnt[c]), nl = local(ctx->q32_cnt[c]);
         if (nh + nl == 0) continue;
         if (timed) PFK_CK(cudaEventRecord(ev[0], st));
         const int os = class_flags(ctx, c);
         const int fp32 = ctx->precision == PFK_PREC_MIXED ? kLaunchFP32 : 0;
-        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, os, st);
-        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, os | fp32, st);
+        int ln = 0;
+        for (int i = 1; i < nlanes; ++i)
+            if (load[i] < load[ln]) ln = i;
+        load[ln] += cost[c];
+        if (nh) ctx->launch[c](ctx->d_quart.p + ctx->q_off[c], nh, a, nk, os, lane_st[ln]);
+        if (nl) ctx->launch[c](ctx->d_quart.p + ctx->q32_off[c], nl, a, nk, os | fp32, lane_st[ln]);
         PFK_CK(cudaGetLastError());
         if (timed) {
             PFK_CK(cudaEventRecord(ev[1], st));
@@ -471,6 +512,10 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
     if (timed) {
         cudaEventDestroy(ev[0]);
         cudaEventDestroy(ev[1]);
+    }
+    for (int i = 1; i < nlanes; ++i) {
+        PFK_CK(cudaEventRecord(ctx->join_ev[i - 1], lane_st[i]));
+        PFK_CK(cudaStreamWaitEvent(st, ctx->join_ev[i - 1], 0));
     }
     return PFK_OK;
 }
@@ -544,6 +589,14 @@ pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
         if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaSetDevice", e));
         e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaStreamCreate", e));
+        e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaEventCreate", e));
+        for (int i = 0; i < kMaxLanes - 1; ++i) {
+            e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+            if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaStreamCreate", e));
+            e = cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaEventCreate", e));
+        }
         ctx->nshell = basis->nshell;
         ctx->L.assign(basis->L, basis->L + basis->nshell);
         ctx->bf_off.resize(basis->nshell);
@@ -619,6 +672,11 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
     ctx->d_Dsh.release();
     for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
         b->release();
+    for (int i = 0; i < kMaxLanes - 1; ++i) {
+        if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+        if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PFK_OK;
@@ -912,6 +970,15 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
     ctx->shard_rank = rank;
     ctx->shard_n = nranks;
     drop_graphs(ctx);
+    return PFK_OK;
+}
+
+pfk_status pfk_set_lanes(pfk_ctx *ctx, int lanes)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (lanes < 1 || lanes > kMaxLanes) return ctx->fail(PFK_ERR_INVALID, "need 1 <= lanes <= 4");
+    if (lanes != ctx->lanes) drop_graphs(ctx);   // captured builds hold the old fork
+    ctx->lanes = lanes;
     return PFK_OK;
 }
 

@@ -124,3 +124,24 @@ def test_autotune_picks_per_class_and_keeps_results(random_basis):
     eng.close()
     assert np.abs(G1 - G0).max() < 1e-11
     assert np.abs(G2 - G1).max() < 1e-13
+
+
+def test_lanes_change_only_the_order_of_additions(random_basis):
+    """Class kernels spread over 1 to 4 streams (pfk_set_lanes): captured
+    device builds and host builds agree to rounding, and an out-of-range
+    lane count is refused."""
+    P = pfk()
+    eng = P.FockEngine(random_basis, engine="auto")
+    Pm = random_density(eng.nbasis, seed=21)
+    eng.set_lanes(1)
+    G1 = eng.fock_rhf(Pm)
+    out = []
+    for lanes in (4, 2, 3, 4):
+        eng.set_lanes(lanes)
+        out.append(eng.fock_rhf(Pm))
+        out.append(eng.fock_rhf(Pm))   # the second build replays the captured graph
+    with pytest.raises(Exception):
+        eng.set_lanes(5)
+    eng.close()
+    for G in out:
+        assert np.abs(G - G1).max() < 1e-12 * max(1.0, np.abs(G1).max())
