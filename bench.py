@@ -353,7 +353,7 @@ def ours_arm(args):
                 "data": "synthetic (seeded water cluster, Basis Set Exchange 6-31G**)",
                 "config": {"workload": WORKLOAD if args.waters == 32 else f"(H2O){args.waters} 6-31G** ({nb} bf)",
                            "nbasis": nb, "tol_eri": 1e-10, "precision": args.precision, "engine": args.engine,
-                           "lanes": args.lanes,
+                           "lanes": args.lanes, "prim_tol": 1e-16,
                            "parallelism": f"quartet-list shards x{world} + NCCL all-reduce of G" if world > 1
                            else "single GPU", "l2": "inputs larger than L2: the screened quartet lists "
                            f"({n_shell * 8 / 1e9:.2f} GB) and primitive-pair data stream from HBM every build",

@@ -161,6 +161,17 @@ pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol);
  * Not in the reference (its loop over quartets is one OpenMP region). */
 pfk_status pfk_set_lanes(pfk_ctx *ctx, int lanes);
 
+/* Primitive screening: every later build of this context skips the
+ * primitive quartets whose bound qp(ab) qp(cd) is below ptol, where qp of a
+ * primitive pair is the largest sqrt|(ab|ab)| over its Cartesian components
+ * for that primitive pair alone (coefficients and norms included).  By the
+ * Cauchy-Schwarz inequality a skipped primitive quartet adds less than ptol
+ * to every integral it touches.  Default 1e-16; 0 evaluates every primitive
+ * pair kept at setup (those that can reach 1e-21 with some partner).
+ * 0 <= ptol <= 1e-10.  Not in the reference, which evaluates every
+ * primitive quartet of a surviving shell quartet. */
+pfk_status pfk_set_primitive_tol(pfk_ctx *ctx, double ptol);
+
 /* Autotuner for engine auto: times every candidate kernel of every class on
  * this context's screened lists (a warm-up pass, then the faster of two timed
  * passes) and keeps the fastest per class for the builds made with engine

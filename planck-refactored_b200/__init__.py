@@ -30,7 +30,7 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_last_error", "pfk_schwarz",
            "pfk_quartet_count", "pfk_quartet_list", "pfk_fock_rhf", "pfk_fock_uhf", "pfk_jk",
            "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
-           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
+           "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_set_primitive_tol", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step"]
 
@@ -81,6 +81,7 @@ def load_library(path=LIB_PATH):
     L.pfk_one_electron.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, vp, vp, vp, c_int]
     L.pfk_set_density_screening.argtypes = [vp, c_dbl]
     L.pfk_set_lanes.argtypes = [vp, c_int]
+    L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
     return L
@@ -219,6 +220,11 @@ class FockEngine:
             if t:
                 out[CLASS_NAMES[c]] = (names[int(choice[c])], t)
         return out
+
+    def set_primitive_tol(self, ptol):
+        """Skip primitive quartets whose Cauchy-Schwarz bound is below ptol
+        (default 1e-16; 0 evaluates them all)."""
+        self._check(self.lib.pfk_set_primitive_tol(self.h, float(ptol)))
 
     def set_lanes(self, lanes):
         """Streams the class kernels of a build are spread over (1 to 4)."""

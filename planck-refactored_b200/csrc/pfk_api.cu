@@ -94,6 +94,7 @@ struct pfk_ctx {
     int shard_rank = 0, shard_n = 1;             // builds evaluate every shard_n-th quartet
 
     double tol = 1e-10, fp32_bound = 1e-8;
+    double prim_tol = kPrimQuartetTol;   // primitive-quartet bound below which builds skip it
     int engine = PFK_ENGINE_OS, precision = PFK_PREC_FP64;
 
     DevBuf<uint2> d_quart;
@@ -201,22 +202,20 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
                     PrimPair p{};
                     p.zeta = zeta;
                     p.inv_zeta = iz;
-                    p.sqrt_zeta = std::sqrt(zeta);
                     p.Px = (alpha * ca[0] + beta * cb[0]) * iz;
                     p.Py = (alpha * ca[1] + beta * cb[1]) * iz;
                     p.Pz = (alpha * ca[2] + beta * cb[2]) * iz;
                     p.PAx = p.Px - ca[0];
                     p.PAy = p.Py - ca[1];
                     p.PAz = p.Pz - ca[2];
-                    p.K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) * b->coef[poff[A] + ia] *
-                          b->coef[poff[B] + ib] * b->norm[poff[A] + ia] * b->norm[poff[B] + ib];
+                    const double K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) *
+                                     b->coef[poff[A] + ia] * b->coef[poff[B] + ib] * b->norm[poff[A] + ia] *
+                                     b->norm[poff[B] + ib];
+                    p.Kz = K * std::sqrt(zeta);
+                    p.qp = 0.0;   // prim_bounds sets it and orders the pair's primitives
                     pp.push_back(p);
                 }
-            std::stable_sort(pp.begin(), pp.end(),
-                             [](const PrimPair &x, const PrimPair &y) { return std::fabs(x.K) > std::fabs(y.K); });
-            pi.nprim_full = (int)pp.size();
-            pi.nprim = 0;
-            while (pi.nprim < pi.nprim_full && std::fabs(pp[pi.nprim].K) >= kPrimPairCut) ++pi.nprim;
+            pi.nprim_full = pi.nprim = (int)pp.size();
             ctx->prims.insert(ctx->prims.end(), pp.begin(), pp.end());
             ctx->pairs.push_back(pi);
             ctx->pair_pc.push_back(pair_class(b->L[A], b->L[B]));
@@ -224,6 +223,48 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
             ctx->pair_lb.push_back(b->L[B]);
         }
     ctx->npairs = (int)ctx->pairs.size();
+}
+
+// Primitive Schwarz bounds (prim_bound_kernel) of the pairs build_pairs made:
+// uploads the pairs, their primitives and the pair ids grouped by pair class
+// (d_ids, npairs entries; cls_begin gets the class starts), computes every
+// qp on the device, brings the primitives back, orders each pair's
+// primitives by qp (descending), keeps in nprim those that can reach
+// kPrimPairFloor with the largest qp of the basis, and uploads the result.
+cudaError_t prim_bounds(pfk_ctx *h, PairInfo *d_pairs, PrimPair *d_prims, int *d_ids, std::vector<int> &cls_begin,
+                        cudaStream_t st)
+{
+    std::vector<int> ids;
+    cls_begin.assign(kPairClasses + 1, 0);
+    for (int x = 0; x < kPairClasses; ++x) {
+        cls_begin[x] = (int)ids.size();
+        for (int p = 0; p < h->npairs; ++p)
+            if (h->pair_pc[p] == x) ids.push_back(p);
+    }
+    cls_begin[kPairClasses] = (int)ids.size();
+    const size_t np = h->prims.size();
+    cudaError_t e = cudaMemcpyAsync(d_pairs, h->pairs.data(), sizeof(PairInfo) * h->npairs, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_prims, h->prims.data(), sizeof(PrimPair) * np, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    for (int x = 0; x < kPairClasses; ++x)
+        launch_prim_bounds(x, d_ids + cls_begin[x], cls_begin[x + 1] - cls_begin[x], d_pairs, d_prims, st);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->prims.data(), d_prims, sizeof(PrimPair) * np, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    double qmax = 0.0;
+    for (const PrimPair &p : h->prims) qmax = std::max(qmax, p.qp);
+    for (PairInfo &pi : h->pairs) {
+        PrimPair *b = h->prims.data() + pi.prim_off;
+        std::stable_sort(b, b + pi.nprim_full, [](const PrimPair &x, const PrimPair &y) { return x.qp > y.qp; });
+        pi.nprim = 0;
+        while (pi.nprim < pi.nprim_full && b[pi.nprim].qp * qmax >= kPrimPairFloor) ++pi.nprim;
+    }
+    e = cudaMemcpyAsync(d_pairs, h->pairs.data(), sizeof(PairInfo) * h->npairs, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_prims, h->prims.data(), sizeof(PrimPair) * np, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
 }
 
 pfk_status upload_pairs(pfk_ctx *ctx)
@@ -456,6 +497,7 @@ pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const 
     a.Kacc1 = K1;
     a.eri_out = eri_out;
     a.tol = ctx->tol;
+    a.ptol = ctx->prim_tol;
     a.nb = ctx->nb;
     a.qstride = ctx->shard_n;
     a.qoffset = ctx->shard_rank;
@@ -621,6 +663,13 @@ pfk_status pfk_create(const pfk_basis_desc *basis, int device, pfk_ctx **out)
         if (e != cudaSuccess) return bail(ctx->cuda_fail("pair tables", e));
         pfk_status s = upload_pairs(ctx);
         if (s != PFK_OK) return bail(s);
+        {
+            DevBuf<int> ids;
+            std::vector<int> cls_begin;
+            e = ids.alloc(std::max(ctx->npairs, 1));
+            if (e == cudaSuccess) e = prim_bounds(ctx, ctx->d_pairs.p, ctx->d_prims.p, ids.p, cls_begin, ctx->stream);
+            if (e != cudaSuccess) return bail(ctx->cuda_fail("primitive bounds", e));
+        }
         for (int c = 0; c < kQuartetClasses; ++c) {
             if (!g_class_launchers[c]) {
                 ctx->err = "class kernel table incomplete (library built without every class unit)";
@@ -973,6 +1022,15 @@ pfk_status pfk_set_shard(pfk_ctx *ctx, int rank, int nranks)
     return PFK_OK;
 }
 
+pfk_status pfk_set_primitive_tol(pfk_ctx *ctx, double ptol)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!(ptol >= 0.0 && ptol <= 1e-10)) return ctx->fail(PFK_ERR_INVALID, "need 0 <= ptol <= 1e-10");
+    if (ptol != ctx->prim_tol) drop_graphs(ctx);   // captured builds hold the old value
+    ctx->prim_tol = ptol;
+    return PFK_OK;
+}
+
 pfk_status pfk_set_lanes(pfk_ctx *ctx, int lanes)
 {
     if (!ctx) return PFK_ERR_STATE;
@@ -1170,18 +1228,11 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
         }                                                                                        \
     } while (0)
 
-    // Schwarz table (the array keeps the previous call's contents: clear it)
-    std::vector<int> ids;
-    std::vector<int> cls_begin(kPairClasses + 1, 0);
-    for (int x = 0; x < kPairClasses; ++x) {
-        cls_begin[x] = (int)ids.size();
-        for (int p = 0; p < h.npairs; ++p)
-            if (h.pair_pc[p] == x) ids.push_back(p);
-    }
-    cls_begin[kPairClasses] = (int)ids.size();
-    PFK_NA_CK(cudaMemcpyAsync(d_pairs, h.pairs.data(), sizeof(PairInfo) * h.npairs, cudaMemcpyHostToDevice, st));
-    PFK_NA_CK(cudaMemcpyAsync(d_prims, h.prims.data(), sizeof(PrimPair) * h.prims.size(), cudaMemcpyHostToDevice, st));
-    PFK_NA_CK(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, st));
+    // primitive bounds (uploads pairs, primitives and the class-grouped pair
+    // ids), then the Schwarz table (the array keeps the previous call's
+    // contents: clear it)
+    std::vector<int> cls_begin;
+    PFK_NA_CK(prim_bounds(&h, d_pairs, d_prims, d_ids, cls_begin, st));
     PFK_NA_CK(cudaMemsetAsync(d_Q, 0, sizeof(double) * nb2, st));
     for (int x = 0; x < kPairClasses; ++x)
         launch_schwarz(x, d_ids + cls_begin[x], cls_begin[x + 1] - cls_begin[x], d_pairs, d_prims, d_Q, nb, st);
@@ -1254,6 +1305,7 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
     a.Jacc = d_J;
     a.Kacc0 = d_K;
     a.tol = tol_eri;
+    a.ptol = kPrimQuartetTol;
     a.nb = nb;
     a.qstride = 1;
     a.qoffset = 0;

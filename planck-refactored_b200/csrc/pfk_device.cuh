@@ -64,18 +64,24 @@ __host__ __device__ constexpr double cart_norm(int L, int i)
 // One primitive pair of an (oriented) shell pair: Gaussian product data.
 // K = (pi/zeta)^1.5 exp(-alpha beta |AB|^2 / zeta) c_a c_b N_a N_b
 // (src/base/types.h:631-674 without the component norms, which are applied
-// per Cartesian component after contraction).
+// per Cartesian component after contraction), stored as Kz = K sqrt(zeta),
+// the factor the quartet prefactor 2 sqrt(rho/pi) K_ab K_cd needs.
+// qp is the pair's primitive Schwarz bound: the largest over its Cartesian
+// components of sqrt|(ab|ab)| for this primitive pair alone, contraction
+// coefficients and component norms included.  By the Cauchy-Schwarz
+// inequality of the Coulomb metric, qp_ab qp_cd bounds what the primitive
+// quartet adds to any normalised component integral of the shell quartet.
 struct __align__(16) PrimPair {
     double zeta, inv_zeta;
     double Px, Py, Pz;
     double PAx, PAy, PAz;   // P - A (A = first centre of the oriented pair)
-    double K, sqrt_zeta;
+    double Kz, qp;
 };
 
 // Shell pair a <= b (shell order), oriented so that L(A) >= L(B).  Its
-// primitive pairs are stored by decreasing |K|; the first nprim have
-// |K| >= kPrimPairCut and are the ones the Fock build evaluates, all
-// nprim_full of them enter the Schwarz table.
+// primitive pairs are stored by decreasing qp; the first nprim have
+// qp * (largest qp of the basis) >= kPrimPairFloor and are the ones the Fock
+// build may evaluate, all nprim_full of them enter the Schwarz table.
 struct __align__(16) PairInfo {
     int prim_off, nprim;     // range in the PrimPair array
     int bf_a, bf_b;          // first basis function of A and of B
@@ -84,12 +90,12 @@ struct __align__(16) PairInfo {
     int nprim_full, pad_;
 };
 
-// Primitive pairs with |K| below this, and primitive quartets with
-// |K_ab K_cd| below kPrimQuartetCut, contribute less than ~1e-16 to any
-// integral (2 sqrt(rho/pi) <= ~1e2 for exponents up to 1e4 and the angular
-// factors stay below ~1e6 where K is not already negligible) and are skipped.
-constexpr double kPrimPairCut = 1e-21;
-constexpr double kPrimQuartetCut = 1e-24;
+// Primitive pairs that cannot reach 1e-21 with any partner are dropped when
+// the pairs are built.  Each build skips the primitive quartets with
+// qp_ab qp_cd below JKArgs::ptol (kPrimQuartetTol unless the context sets
+// another value): each adds less than ptol to every integral it touches.
+constexpr double kPrimPairFloor = 1e-21;
+constexpr double kPrimQuartetTol = 1e-16;
 
 struct JKArgs {
     const PairInfo *__restrict__ pairs;
@@ -113,6 +119,8 @@ struct JKArgs {
     // that shell-pair block of every density of the build
     const float *__restrict__ Dsh;
     double dtol;
+    // primitive quartets with qp_ab qp_cd < ptol are skipped (0: none)
+    double ptol;
 };
 
 // ---------------------------------------------------------------------------
@@ -258,8 +266,9 @@ __device__ __forceinline__ QuartetScalars quartet_scalars(const PrimPair &p, con
     s.rho = p.zeta * q.zeta * s.rdelta;
     const double PQx = p.Px - q.Px, PQy = p.Py - q.Py, PQz = p.Pz - q.Pz;
     s.T = s.rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-    // 2 sqrt(rho / pi) K_ab K_cd  (rys.cpp:415), sqrt(rho) = sqrt(zeta) sqrt(eta) / sqrt(delta)
-    s.pref = 1.1283791670955125739 * (p.sqrt_zeta * q.sqrt_zeta * rs) * (p.K * q.K);
+    // 2 sqrt(rho / pi) K_ab K_cd  (rys.cpp:415), sqrt(rho) = sqrt(zeta) sqrt(eta) / sqrt(delta),
+    // with sqrt(zeta) and sqrt(eta) folded into Kz
+    s.pref = 1.1283791670955125739 * (p.Kz * q.Kz) * rs;
     s.zinv = p.inv_zeta;
     s.einv = q.inv_zeta;
     const double fp = -q.zeta * s.rdelta, fq = p.zeta * s.rdelta;  // W-P = fp PQ, W-Q = fq PQ
@@ -274,7 +283,7 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
     const double2 x0 = __ldg(v), x1 = __ldg(v + 1), x2 = __ldg(v + 2), x3 = __ldg(v + 3), x4 = __ldg(v + 4);
     PrimPair p;
     p.zeta = x0.x; p.inv_zeta = x0.y; p.Px = x1.x; p.Py = x1.y; p.Pz = x2.x;
-    p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.K = x4.x; p.sqrt_zeta = x4.y;
+    p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.Kz = x4.x; p.qp = x4.y;
     return p;
 }
 

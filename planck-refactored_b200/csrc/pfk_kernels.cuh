@@ -310,11 +310,13 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
+    const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
     for (int jp = 0; jp < pk.nprim; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
             const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
+            if (p.qp * q.qp < args.ptol) break;   // bras sorted by qp
             const QuartetScalars s = quartet_scalars(p, q);
             double u[NR], w[NR];
             rys_roots<NR>(s.T, u, w);
@@ -412,11 +414,13 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
+    const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
     for (int jp = 0; jp < pk.nprim; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
             const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
+            if (p.qp * q.qp < args.ptol) break;   // bras sorted by qp
             const QuartetScalars s = quartet_scalars(p, q);
             for (int task = lane; task < 3 * NR; task += TEAM) {
                 const int r = task / 3, axis = task - 3 * r;
@@ -482,12 +486,38 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
 // Schwarz diagonal (ab|ab) per shell pair of class (LA, LB): Q(i,j) for all
 // component pairs (os.cpp:1703-1752, rys.cpp:509-556).
 // ---------------------------------------------------------------------------
+// Adds the diagonal (ab|ab) of one primitive quartet (p, q) of shell pair pb
+// to acc[ia * NB + ib] (unnormalised Cartesian components).
+template <int LA, int LB>
+__device__ __forceinline__ void diag_add(const PrimPair &p, const PrimPair &q, const PairInfo &pb, double *acc)
+{
+    using S = ClassShape<LA, LB, LA, LB>;
+    constexpr int NA = S::NA, NB = S::NB, NR = S::NR, NI = S::NI;
+    const QuartetScalars s = quartet_scalars(p, q);
+    double u[NR], w[NR];
+    rys_roots<NR>(s.T, u, w);
+    for (int r = 0; r < NR; ++r) {
+        const double ur = u[r];
+        const double B00 = 0.5 * s.rdelta * ur;
+        const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
+        const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
+        double gx[NI], gy[NI], gz[NI];
+        axis_table<LA, LB, LA, LB, double>(p.PAx + ur * s.WPx, q.PAx + ur * s.WQx, B00, B10, B01, pb.ABx, pb.ABx, w[r] * s.pref, gx);
+        axis_table<LA, LB, LA, LB, double>(p.PAy + ur * s.WPy, q.PAy + ur * s.WQy, B00, B10, B01, pb.ABy, pb.ABy, 1.0, gy);
+        axis_table<LA, LB, LA, LB, double>(p.PAz + ur * s.WPz, q.PAz + ur * s.WQz, B00, B10, B01, pb.ABz, pb.ABz, 1.0, gz);
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+                acc[ia * NB + ib] += gx[S::ax(ia, ib, ia, ib)] * gy[S::ay(ia, ib, ia, ib)] * gz[S::az(ia, ib, ia, ib)];
+    }
+}
+
 template <int LA, int LB>
 __global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pair_ids, int n, const PairInfo *__restrict__ pairs,
                                                      const PrimPair *__restrict__ prims, double *Qao, int nb)
 {
-    using S = ClassShape<LA, LB, LA, LB>;
-    constexpr int NA = S::NA, NB = S::NB, NR = S::NR, NI = S::NI;
+    constexpr int NA = ncart(LA), NB = ncart(LB);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const PairInfo pb = pairs[pair_ids[t]];
@@ -496,27 +526,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pai
     for (int c = 0; c < NA * NB; ++c) acc[c] = 0.0;
     for (int ip = 0; ip < pb.nprim_full; ++ip) {
         const PrimPair p = load_prim(prims, pb.prim_off + ip);
-        for (int jp = 0; jp < pb.nprim_full; ++jp) {
-            const PrimPair q = load_prim(prims, pb.prim_off + jp);
-            const QuartetScalars s = quartet_scalars(p, q);
-            double u[NR], w[NR];
-            rys_roots<NR>(s.T, u, w);
-            for (int r = 0; r < NR; ++r) {
-                const double ur = u[r];
-                const double B00 = 0.5 * s.rdelta * ur;
-                const double B10 = 0.5 * s.zinv * (1.0 - s.rho * s.zinv * ur);
-                const double B01 = 0.5 * s.einv * (1.0 - s.rho * s.einv * ur);
-                double gx[NI], gy[NI], gz[NI];
-                axis_table<LA, LB, LA, LB, double>(p.PAx + ur * s.WPx, q.PAx + ur * s.WQx, B00, B10, B01, pb.ABx, pb.ABx, w[r] * s.pref, gx);
-                axis_table<LA, LB, LA, LB, double>(p.PAy + ur * s.WPy, q.PAy + ur * s.WQy, B00, B10, B01, pb.ABy, pb.ABy, 1.0, gy);
-                axis_table<LA, LB, LA, LB, double>(p.PAz + ur * s.WPz, q.PAz + ur * s.WQz, B00, B10, B01, pb.ABz, pb.ABz, 1.0, gz);
-#pragma unroll
-                for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-                    for (int ib = 0; ib < NB; ++ib)
-                        acc[ia * NB + ib] += gx[S::ax(ia, ib, ia, ib)] * gy[S::ay(ia, ib, ia, ib)] * gz[S::az(ia, ib, ia, ib)];
-            }
-        }
+        for (int jp = 0; jp < pb.nprim_full; ++jp) diag_add<LA, LB>(p, load_prim(prims, pb.prim_off + jp), pb, acc);
     }
 #pragma unroll
     for (int ia = 0; ia < NA; ++ia)
@@ -528,6 +538,36 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const int *__restrict__ pai
             Qao[(size_t)i * nb + j] = q;
             Qao[(size_t)j * nb + i] = q;
         }
+}
+
+// Primitive Schwarz bound of every primitive pair of the listed shell pairs:
+// prims[k].qp = max over components of sqrt|N_a^2 N_b^2 (ab|ab)| for
+// primitive pair k alone (one thread per shell pair; the pairs' primitive
+// ranges are disjoint).
+template <int LA, int LB>
+__global__ void __launch_bounds__(64) prim_bound_kernel(const int *__restrict__ pair_ids, int n,
+                                                        const PairInfo *__restrict__ pairs, PrimPair *prims)
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const PairInfo pb = pairs[pair_ids[t]];
+    for (int ip = 0; ip < pb.nprim_full; ++ip) {
+        const PrimPair p = prims[pb.prim_off + ip];
+        double acc[NA * NB];
+#pragma unroll
+        for (int c = 0; c < NA * NB; ++c) acc[c] = 0.0;
+        diag_add<LA, LB>(p, p, pb, acc);
+        double m = 0.0;
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) {
+                const double nrm = cart_norm(LA, ia) * cart_norm(LB, ib);
+                m = fmax(m, fabs(acc[ia * NB + ib] * nrm * nrm));
+            }
+        prims[pb.prim_off + ip].qp = sqrt(m);
+    }
 }
 
 }  // namespace pfk
@@ -639,11 +679,13 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
+    const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
     for (int jp = 0; jp < pk.nprim; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
             const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
+            if (p.qp * q.qp < args.ptol) break;   // bras sorted by qp
             const QuartetScalars s = quartet_scalars(p, q);
             for (int task = lane; task < 3 * NR; task += TEAM) {
                 const int r = task / 3, axis = task - 3 * r;

@@ -357,11 +357,13 @@ __global__ void __launch_bounds__(128, MINB) eri_os_kernel(const uint2 *__restri
     // pair, so bra loads are broadcasts).  Loading the next bra primitive
     // ahead of the current one was measured slower: its registers cost more
     // occupancy than the latency it hides.
+    const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
     for (int jp = 0; jp < pk.nprim; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
+        if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
             const PrimPair p = load_prim(args.prims, pb.prim_off + ip);
-            if (fabs(p.K * q.K) < kPrimQuartetCut) break;   // bras sorted by |K|
+            if (p.qp * q.qp < args.ptol) break;   // bras sorted by qp
             const QuartetScalars s = quartet_scalars(p, q);
             double Fm[L + 1];
             boys_fm<L>(s.T, Fm);

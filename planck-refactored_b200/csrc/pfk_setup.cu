@@ -19,6 +19,30 @@ static void launch_schwarz_pc(const int *ids, int n, const PairInfo *pairs, cons
     schwarz_kernel<pc_la(PC), pc_lb(PC)><<<(n + 63) / 64, 64, 0, st>>>(ids, n, pairs, prims, Q, nb);
 }
 
+template <int PC>
+static void launch_prim_bounds_pc(const int *ids, int n, const PairInfo *pairs, PrimPair *prims, cudaStream_t st)
+{
+    if (n <= 0) return;
+    prim_bound_kernel<pc_la(PC), pc_lb(PC)><<<(n + 63) / 64, 64, 0, st>>>(ids, n, pairs, prims);
+}
+
+void launch_prim_bounds(int pc, const int *ids, int n, const PairInfo *pairs, PrimPair *prims, cudaStream_t st)
+{
+    switch (pc) {
+    case 0: launch_prim_bounds_pc<0>(ids, n, pairs, prims, st); break;
+    case 1: launch_prim_bounds_pc<1>(ids, n, pairs, prims, st); break;
+    case 2: launch_prim_bounds_pc<2>(ids, n, pairs, prims, st); break;
+    case 3: launch_prim_bounds_pc<3>(ids, n, pairs, prims, st); break;
+    case 4: launch_prim_bounds_pc<4>(ids, n, pairs, prims, st); break;
+    case 5: launch_prim_bounds_pc<5>(ids, n, pairs, prims, st); break;
+    case 6: launch_prim_bounds_pc<6>(ids, n, pairs, prims, st); break;
+    case 7: launch_prim_bounds_pc<7>(ids, n, pairs, prims, st); break;
+    case 8: launch_prim_bounds_pc<8>(ids, n, pairs, prims, st); break;
+    case 9: launch_prim_bounds_pc<9>(ids, n, pairs, prims, st); break;
+    default: break;
+    }
+}
+
 void launch_schwarz(int pc, const int *ids, int n, const PairInfo *pairs, const PrimPair *prims, double *Q, int nb,
                     cudaStream_t st)
 {

@@ -8,6 +8,7 @@ namespace pfk {
 
 void launch_schwarz(int pc, const int *ids, int n, const PairInfo *pairs, const PrimPair *prims, double *Q, int nb,
                     cudaStream_t st);
+void launch_prim_bounds(int pc, const int *ids, int n, const PairInfo *pairs, PrimPair *prims, cudaStream_t st);
 cudaError_t count_quartets(const double *qX, int nX, const double *qY, int nY, int diag, double tol, double bound,
                            long long *cnt_hi, long long *cnt_lo, cudaStream_t st);
 cudaError_t exclusive_scan(const long long *in, long long *out, int n, void *tmp, size_t &tmp_bytes, cudaStream_t st);

@@ -145,3 +145,30 @@ def test_lanes_change_only_the_order_of_additions(random_basis):
     eng.close()
     for G in out:
         assert np.abs(G - G1).max() < 1e-12 * max(1.0, np.abs(G1).max())
+
+
+def test_primitive_screening_bound_holds(random_basis):
+    """pfk_set_primitive_tol: builds with the default bound (1e-16), with
+    every primitive (0) and with 1e-12 agree to within what the skipped
+    primitive quartets can add (each below ptol per integral), the default
+    build stays within 1e-10 of the oracle, and values outside [0, 1e-10] are
+    refused."""
+    P = pfk()
+    shells = random_basis
+    ob = oracle.Basis(shells)
+    eri_o, _ = ob.eri_tensor(1e-10, oracle.OS)
+    eng = P.FockEngine(shells, engine="os")
+    Pm = random_density(eng.nbasis, seed=23)
+    G_o = oracle.fock_rhf_tensor(eri_o, Pm)
+    G_def = eng.fock_rhf(Pm)
+    eng.set_primitive_tol(0.0)
+    G_all = eng.fock_rhf(Pm)
+    eng.set_primitive_tol(1e-12)
+    G_loose = eng.fock_rhf(Pm)
+    for bad in (-1.0, 1e-9, float("nan")):
+        with pytest.raises(Exception):
+            eng.set_primitive_tol(bad)
+    eng.close()
+    assert np.abs(G_def - G_o).max() < 1e-10
+    assert np.abs(G_def - G_all).max() < 1e-11
+    assert np.abs(G_loose - G_all).max() < 1e-7
