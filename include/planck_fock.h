@@ -256,6 +256,67 @@ pfk_status pfk_mlp_train_step(pfk_mlp *m, const float *X, const float *T, int n,
 pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const double *dP, double *dG, double tol_eri,
                                 void *stream);
 
+/* ---- Checkpoint files (.hfchk, format version 6) ----------------------
+ * The reference's restart file (src/io/checkpoint.h:11-72), so that a density
+ * made here -- a learned guess, or a converged GPU SCF -- restarts the
+ * reference with `guess density`, and a reference checkpoint restarts this
+ * library's driver.  Host code; no GPU is needed.  Files are host byte
+ * order with IEEE-754 doubles, like the reference's.  Every nbasis x nbasis
+ * array below is column-major (element (i, j) at i + nbasis * j), the layout
+ * of the reference's Eigen matrices; for the symmetric ones it does not
+ * matter. */
+
+/* Molecule and run data of a checkpoint (the Calculator fields that
+ * Checkpoint::save writes, checkpoint.cpp:356-379). */
+typedef struct {
+    int natoms;
+    const int *atomic_numbers;    /* [natoms] */
+    const double *coords_bohr;    /* [3*natoms]: x0 y0 z0 x1 y1 z1 ... */
+    int charge;
+    unsigned int multiplicity;
+    const char *basis_name;       /* NUL-terminated, at most 4096 bytes */
+    double total_energy;
+    double nuclear_repulsion;
+    int converged;                /* 0 or 1 */
+    int has_opt_coords;           /* 0 or 1 */
+} pfk_checkpoint_meta;
+
+/* One spin channel (SpinChannel: density, Fock matrix, orbital energies
+ * [nbasis], MO coefficients with MO j in column j). */
+typedef struct {
+    const double *density;
+    const double *fock;
+    const double *mo_energies;
+    const double *mo_coefficients;
+} pfk_spin_channel;
+
+/* Write a checkpoint as Checkpoint::save does (checkpoint.cpp:347-489):
+ * header, molecule, S, H, the alpha channel, the beta channel when beta is
+ * non-NULL (UHF/ROHF), no CASSCF data, and the shell and basis-function
+ * tables of `basis`, whose Cartesian function count is the file's nbasis.
+ * An RHF channel holds the total density; a UHF or ROHF reader of an RHF
+ * file builds its spin densities from the leading MO columns, so list the
+ * occupied orbitals first. */
+pfk_status pfk_checkpoint_write(const char *path, const pfk_checkpoint_meta *meta, const pfk_basis_desc *basis,
+                                const double *S, const double *H, const pfk_spin_channel *alpha,
+                                const pfk_spin_channel *beta);
+
+/* Density restart, as Checkpoint::load with load_1e_matrices = false
+ * (checkpoint.cpp:491-663): the same checks and error messages (magic,
+ * version 2..6, nbasis, size limits, truncation), then the stored densities
+ * adapted to the target like adapt_restart_spin_state
+ * (checkpoint.cpp:294-336): UHF file and UHF target -> Pa, Pb as stored;
+ * UHF file, RHF target -> Pa = P_alpha + P_beta; RHF file, RHF target -> Pa
+ * = the stored density; RHF file, UHF target -> Pa, Pb from the first
+ * n_alpha / n_beta MO columns.  Pb may be NULL for an RHF target.  The
+ * stored total energy and whether the file is spin-resolved come back in
+ * the optional last two arguments. */
+pfk_status pfk_checkpoint_read_density(const char *path, int nbasis, int target_uhf, int n_alpha, int n_beta,
+                                       double *Pa, double *Pb, double *total_energy, int *checkpoint_uhf);
+
+/* Message of the last failed checkpoint call on this thread. */
+const char *pfk_checkpoint_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,8 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_fock_rhf_device", "pfk_eri_tensor", "pfk_class_stats", "pfk_set_shard", "pfk_measure_fma_peak",
            "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_set_primitive_tol", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
-           "pfk_mlp_train_step"]
+           "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
+           "pfk_checkpoint_last_error"]
 
 _lib = None
 
@@ -65,6 +66,8 @@ def load_library(path=LIB_PATH):
     L.pfk_set_options.argtypes = [vp, c_dbl, c_int, c_int, c_dbl]
     L.pfk_nbasis.argtypes = [vp]
     L.pfk_last_error.restype = ctypes.c_char_p
+    L.pfk_checkpoint_last_error.restype = ctypes.c_char_p
+    L.pfk_checkpoint_last_error.argtypes = []
     L.pfk_last_error.argtypes = [vp]
     L.pfk_schwarz.argtypes = [vp, vp]
     L.pfk_quartet_count.argtypes = [vp, ctypes.POINTER(c_ll), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(c_ll)]
@@ -316,4 +319,4 @@ def _compute_2e_fock_uhf(eng, Pa, Pb, nbasis, engine="os", tol_eri=1e-10, sym_op
     """(G_alpha, G_beta) (base.h:75-93)."""
     _prepare(eng, nbasis, engine, tol_eri, sym_ops)
     return eng.fock_uhf(Pa, Pb)
-from . import guess, mlp, scf  # noqa: E402,F401  (RHF driver and learned guess; import this package lazily)
+from . import checkpoint, guess, mlp, scf  # noqa: E402,F401  (RHF driver and learned guess; import this package lazily)

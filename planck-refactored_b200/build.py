@@ -31,6 +31,7 @@ DEPS = {
     "pfk_api.cu": DEVICE_DEPS + ["pfk_setup.h", "../../include/planck_fock.h"],
     "pfk_onee.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_os.cuh"],
     "pfk_mlp.cu": ["../../include/planck_fock.h"],
+    "pfk_checkpoint.cu": ["../../include/planck_fock.h"],
 }
 
 
@@ -44,7 +45,7 @@ def _units():
     units = [("pfk_classes.cu", f"classes_{b}_{e}.o", [f"-DPFK_CLASS_BEGIN={b}", f"-DPFK_CLASS_END={e}"])
              for b, e in reversed(CLASS_UNITS)]
     units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", []), ("pfk_onee.cu", "onee.o", []),
-              ("pfk_mlp.cu", "mlp.o", [])]
+              ("pfk_mlp.cu", "mlp.o", []), ("pfk_checkpoint.cu", "checkpoint.o", [])]
     return units
 
 

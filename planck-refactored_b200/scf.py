@@ -157,6 +157,7 @@ class System:
     def __init__(self, atoms, basis_name, library, device=0, engine="os", precision="fp64", fp32_bound=1e-8):
         from . import FockEngine, one_electron, shells_for
         self.mol, self.shells = shells_for(atoms, basis_name, library)
+        self.basis_name = basis_name
         S, T, V = one_electron(self.shells, self.mol.coords, self.mol.Z, device)
         self.S, self.H = S, T + V
         self.enuc = nuclear_repulsion(self.mol.coords, self.mol.Z)

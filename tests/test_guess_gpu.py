@@ -65,3 +65,36 @@ def test_shipped_model_reduces_iterations():
     assert res["all_converged"]
     assert res["max_abs_dE_Eh"] < 1e-8
     assert res["mean_iterations_learned"] < res["mean_iterations_default"]
+
+
+def test_learned_guess_through_a_checkpoint_file(tmp_path):
+    """The hook's density written as a .hfchk (checkpoint.save_guess) and
+    read back as the reference's `guess density` restart reads it: the
+    density comes back bit for bit, and the SCF started from the file takes
+    the same iterations to the same energy as the SCF started from the hook
+    directly.  A converged SCF written and restarted converges at once."""
+    P = pfk()
+    T = _trainer()
+    model = P.guess.GuessModel.load(MODEL)
+    nc, atoms = T.conformer(7, 8, 9, 4_000_000)
+    sysm = P.scf.System(atoms, "6-31g*", basis_library())
+    nb = sysm.H.shape[0]
+    path = os.path.join(tmp_path, "guess.hfchk")
+    P0, G0, info = P.checkpoint.save_guess(path, model, sysm)
+    Pf, _, e_first, uhf = P.checkpoint.read_density(path, nb)
+    assert not uhf and np.array_equal(Pf, P0)
+    assert e_first == (info["E_first_learned"] if info["accepted"] else info["E_first_default"])
+    r_hook = sysm.run(P0=P0)
+    r_file = sysm.run(P0=Pf)
+    assert r_hook["converged"] and r_file["converged"]
+    assert r_file["iterations"] == r_hook["iterations"]
+    assert abs(r_file["energy"] - r_hook["energy"]) < 1e-10
+    conv = os.path.join(tmp_path, "converged.hfchk")
+    P.checkpoint.write(conv, sysm, r_file["P"], energy=r_file["energy"], converged=True)
+    Pc, _, e, _ = P.checkpoint.read_density(conv, nb)
+    r_restart = sysm.run(P0=Pc)
+    sysm.close()
+    model.close()
+    assert e == r_file["energy"]
+    assert r_restart["converged"] and r_restart["iterations"] <= 3
+    assert abs(r_restart["energy"] - r_file["energy"]) < 1e-9
