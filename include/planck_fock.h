@@ -125,6 +125,19 @@ pfk_status pfk_fock_rhf_device(pfk_ctx *ctx, const double *dP, double *dG, void 
  * (_compute_2e, os.cpp:1755-1829).  Host buffer of nb^4 doubles. */
 pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri);
 
+/* AO -> MO transform of the stored tensor, the consumer behind MP2 and the
+ * stability analysis (transform_eri, src/post_hf/integrals.cpp:63-134):
+ *   out[i][a][j][b] = sum_{mu nu lam sig} C1(mu,i) C2(nu,a) C3(lam,j) C4(sig,b)
+ *                     (mu nu|lam sig),
+ * row-major n1 x n2 x n3 x n4 in a host buffer.  C_k are host nbasis x n_k
+ * matrices, column-major (the reference's Eigen MO blocks), 1 <= n_k <=
+ * nbasis.  The AO tensor is built on the device by the class kernels
+ * (as pfk_eri_tensor, nbasis <= 180) and the four quarter transforms run
+ * there as FP64 GEMMs (cuBLAS); nothing of size nbasis^4 crosses to the
+ * host. */
+pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3,
+                            int n3, const double *C4, int n4, double *out);
+
 /* Per-class work of one build over the 55 classes (ss|ss)..(ff|ff):
  * screened shell quartets, primitive quartets (sum of K_ab * K_cd), and --
  * when ms55 is non-null -- the device time of each class's kernel in a

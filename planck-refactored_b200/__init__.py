@@ -33,7 +33,7 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_set_primitive_tol", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
-           "pfk_checkpoint_last_error"]
+           "pfk_checkpoint_last_error", "pfk_mo_transform"]
 
 _lib = None
 
@@ -84,6 +84,7 @@ def load_library(path=LIB_PATH):
     L.pfk_one_electron.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, vp, vp, vp, c_int]
     L.pfk_set_density_screening.argtypes = [vp, c_dbl]
     L.pfk_set_lanes.argtypes = [vp, c_int]
+    L.pfk_mo_transform.argtypes = [vp, vp, c_int, vp, c_int, vp, c_int, vp, c_int, vp]
     L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
@@ -197,6 +198,18 @@ class FockEngine:
         eri = np.zeros((nb, nb, nb, nb))
         self._check(self.lib.pfk_eri_tensor(self.h, _p(eri)))
         return eri
+
+    def mo_transform(self, C1, C2, C3, C4):
+        """(C1 C2 | C3 C4) MO integrals, shape (n1, n2, n3, n4), from the
+        device-resident AO tensor (pfk_mo_transform; nbasis <= 180).  C_k are
+        nbasis x n_k arrays of MO coefficients."""
+        Cs = [np.asarray(C, dtype=np.float64).reshape(self.nbasis, -1) for C in (C1, C2, C3, C4)]
+        cm = [np.ascontiguousarray(C.T) for C in Cs]   # column-major storage
+        n = [C.shape[1] for C in Cs]
+        out = np.zeros(n)
+        self._check(self.lib.pfk_mo_transform(self.h, _p(cm[0]), n[0], _p(cm[1]), n[1], _p(cm[2]), n[2],
+                                              _p(cm[3]), n[3], _p(out)))
+        return out
 
     def class_stats(self, timed=True):
         """{class name: (shell quartets, primitive quartets, ms)} for non-empty classes."""
@@ -319,4 +332,4 @@ def _compute_2e_fock_uhf(eng, Pa, Pb, nbasis, engine="os", tol_eri=1e-10, sym_op
     """(G_alpha, G_beta) (base.h:75-93)."""
     _prepare(eng, nbasis, engine, tol_eri, sym_ops)
     return eng.fock_uhf(Pa, Pb)
-from . import checkpoint, guess, mlp, scf  # noqa: E402,F401  (RHF driver and learned guess; import this package lazily)
+from . import checkpoint, guess, mlp, mp2, scf  # noqa: E402,F401  (RHF driver and learned guess; import this package lazily)

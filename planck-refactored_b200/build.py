@@ -79,7 +79,7 @@ def build(jobs=None, force=False, verbose=False):
                 logs[futs[f][1]] = f.result()
     objs = [os.path.join(BUILD, o) for _, o, _ in _units()]
     if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcublas"]
         subprocess.check_call(cmd)
     return LIB, logs
 

@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <cublas_v2.h>
+
 #include "../../include/planck_fock.h"
 #include "pfk_internal.h"
 #include "pfk_setup.h"
@@ -67,6 +69,7 @@ struct pfk_ctx {
     int lanes = kMaxLanes;
     cudaStream_t side[kMaxLanes - 1] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes - 1] = {};
+    cublasHandle_t blas = nullptr;   // created by the first pfk_mo_transform
 
     int nshell = 0, nb = 0;
     std::vector<int> L, bf_off;
@@ -726,6 +729,7 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
         if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
     }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->blas) cublasDestroy(ctx->blas);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PFK_OK;
@@ -925,6 +929,74 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
     if (s != PFK_OK) return s;
     PFK_CK(cudaMemcpyAsync(eri, d.p, sizeof(double) * n4, cudaMemcpyDeviceToHost, ctx->stream));
     PFK_CK(cudaStreamSynchronize(ctx->stream));
+    return PFK_OK;
+}
+
+// AO -> MO transform of the stored tensor (transform_eri,
+// src/post_hf/integrals.cpp:63-134): the dense AO tensor from the class
+// kernels' tensor mode, then the four quarter transforms as FP64 GEMMs on
+// the device.  Row-major tensors; the C_k are nb x n_k column-major.
+//   T1[i][nls]  = sum_m C1(m,i) E[m][nls]     one GEMM, (nb^3 x nb)(nb x n1)
+//   T2[i][a][ls] = sum_n C2(n,a) T1[i][n][ls] n1 GEMMs, (nb^2 x nb)(nb x n2)
+//   T3[ia][j][s] = sum_l C3(l,j) T2[ia][l][s] n1 n2 GEMMs, (nb x nb)(nb x n3)
+//   out[iaj][b]  = sum_s T3[iaj][s] C4(s,b)  one GEMM, (n4 x nb)(nb x n1 n2 n3)
+pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3,
+                            int n3, const double *C4, int n4, double *out)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!C1 || !C2 || !C3 || !C4 || !out) return ctx->fail(PFK_ERR_INVALID, "null argument");
+    const int nb = ctx->nb;
+    if (n1 < 1 || n2 < 1 || n3 < 1 || n4 < 1 || n1 > nb || n2 > nb || n3 > nb || n4 > nb)
+        return ctx->fail(PFK_ERR_INVALID, "need 1 <= n_k <= nbasis");
+    if (nb > 180) return ctx->fail(PFK_ERR_UNSUPPORTED, "dense tensor limited to 180 basis functions (8.4 GB)");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    if (!ctx->blas) {
+        if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return ctx->fail(PFK_ERR_CUDA, "cublasCreate failed");
+    }
+    if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return ctx->fail(PFK_ERR_CUDA, "cublasSetStream failed");
+    const size_t b = nb, b2 = b * b, b3 = b2 * b;
+    DevBuf<double> E, T1, T2, T3, O, dC[4];
+    const double *hC[4] = {C1, C2, C3, C4};
+    const int nk[4] = {n1, n2, n3, n4};
+    for (int k = 0; k < 4; ++k) {
+        PFK_CK(dC[k].alloc(b * nk[k]));
+        PFK_CK(cudaMemcpyAsync(dC[k].p, hC[k], sizeof(double) * b * nk[k], cudaMemcpyHostToDevice, st));
+    }
+    PFK_CK(E.alloc(b2 * b2));
+    PFK_CK(cudaMemsetAsync(E.p, 0, sizeof(double) * b2 * b2, st));
+    pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, E.p, st, false);
+    if (s != PFK_OK) return s;
+    const double one = 1.0, zero = 0.0;
+    auto ck = [&](cublasStatus_t r, const char *what) {
+        return r == CUBLAS_STATUS_SUCCESS ? PFK_OK : ctx->fail(PFK_ERR_CUDA, std::string(what) + " failed");
+    };
+    PFK_CK(T1.alloc(b3 * n1));
+    s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)b3, n1, nb, &one, E.p, (int)b3, dC[0].p, nb, &zero,
+                       T1.p, (int)b3),
+           "quarter transform 1 (cublasDgemm)");
+    if (s != PFK_OK) return s;
+    E.release();
+    PFK_CK(T2.alloc(b2 * n1 * n2));
+    s = ck(cublasDgemmStridedBatched(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)b2, n2, nb, &one, T1.p, (int)b2,
+                                     (long long)b3, dC[1].p, nb, 0, &zero, T2.p, (int)b2, (long long)b2 * n2, n1),
+           "quarter transform 2 (cublasDgemmStridedBatched)");
+    if (s != PFK_OK) return s;
+    T1.release();
+    PFK_CK(T3.alloc(b * n1 * n2 * n3));
+    s = ck(cublasDgemmStridedBatched(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, n3, nb, &one, T2.p, nb, (long long)b2,
+                                     dC[2].p, nb, 0, &zero, T3.p, nb, (long long)b * n3, n1 * n2),
+           "quarter transform 3 (cublasDgemmStridedBatched)");
+    if (s != PFK_OK) return s;
+    T2.release();
+    const size_t no = (size_t)n1 * n2 * n3 * n4;
+    PFK_CK(O.alloc(no));
+    s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, n4, n1 * n2 * n3, nb, &one, dC[3].p, nb, T3.p, nb, &zero,
+                       O.p, n4),
+           "quarter transform 4 (cublasDgemm)");
+    if (s != PFK_OK) return s;
+    PFK_CK(cudaMemcpyAsync(out, O.p, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
+    PFK_CK(cudaStreamSynchronize(st));
     return PFK_OK;
 }
 

@@ -150,6 +150,53 @@ def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, 
             "history": history, "first_energy": E_first}
 
 
+def uhf(engine, H, S, enuc, n_alpha, n_beta, P0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8):
+    """UHF to convergence (the loop of run_uhf, src/scf/scf.cpp:467-930) on
+    FockEngine.fock_uhf (Ga = J(Pa+Pb) - K(Pa), Gb = J(Pa+Pb) - K(Pb)).
+    Guess: per spin, the n_s lowest eigenvectors of X^T H X
+    (scf.cpp:505-511), or P0 = (Pa, Pb).  Per iteration
+    E = 1/2 sum[(Pa + Pb) H + Pa Fa + Pb Fb] + E_nuc; one Pulay extrapolation
+    of (Fa, Fb) with the joint error (X^T (Fs Ps S - S Ps Fs) X)_s; converged
+    when |dE| and the rms and max of both density steps are below the
+    thresholds, not before the second iteration.  Returns energy,
+    iterations, converged, Pa, Pb, Ca, Cb, eps_a, eps_b, history."""
+    nb = H.shape[0]
+    X = orthogonaliser(S)
+    if P0 is None:
+        _, Cp = np.linalg.eigh(X.T @ H @ X)
+        C = X @ Cp
+        Pa, Pb = C[:, :n_alpha] @ C[:, :n_alpha].T, C[:, :n_beta] @ C[:, :n_beta].T
+    else:
+        Pa, Pb = (np.array(p, dtype=np.float64) for p in P0)
+    max_iter = max_iter or max_cycles(nb)
+    diis = Pulay(diis_depth)
+    E_prev, history = 0.0, []
+    for it in range(1, max_iter + 1):
+        Ga, Gb = engine.fock_uhf(Pa, Pb)
+        Fa, Fb = H + Ga, H + Gb
+        E = 0.5 * float(np.sum((Pa + Pb) * H + Pa * Fa + Pb * Fb)) + enuc
+        err = np.stack([X.T @ (F @ Ps @ S - S @ Ps @ F) @ X for F, Ps in ((Fa, Pa), (Fb, Pb))])
+        diis.add(np.stack([Fa, Fb]), err)
+        Fx = diis.fock()
+        out = []
+        for F, n in ((Fx[0], n_alpha), (Fx[1], n_beta)):
+            eps, Cp = np.linalg.eigh(X.T @ F @ X)
+            C = X @ Cp
+            out.append((eps, C, C[:, :n] @ C[:, :n].T))
+        (eps_a, Ca, Pan), (eps_b, Cb, Pbn) = out
+        dPa, dPb = Pan - Pa, Pbn - Pb
+        dE = abs(E - E_prev)
+        dmax = max(float(np.abs(dPa).max()), float(np.abs(dPb).max()))
+        drms = max(float(np.sqrt(np.mean(dPa * dPa))), float(np.sqrt(np.mean(dPb * dPb))))
+        history.append((it, E, dE, drms, dmax))
+        Pa, Pb, E_prev = Pan, Pbn, E
+        if it > 1 and dE < tol_e and drms < tol_d and dmax < tol_d:
+            return {"energy": E, "iterations": it, "converged": True, "Pa": Pa, "Pb": Pb, "Ca": Ca, "Cb": Cb,
+                    "eps_a": eps_a, "eps_b": eps_b, "history": history}
+    return {"energy": E_prev, "iterations": max_iter, "converged": False, "Pa": Pa, "Pb": Pb, "Ca": Ca, "Cb": Cb,
+            "eps_a": eps_a, "eps_b": eps_b, "history": history}
+
+
 class System:
     """A molecule on one GPU: basis shells, one-electron matrices from the
     device (pfk_one_electron), nuclear repulsion and a FockEngine."""

@@ -13,8 +13,12 @@ Writes, next to this script:
                           Fortran D exponents, SP split into S then P, shell
                           scale factor multiplied into the coefficients).
   regression_cases.json   The reference's RHF regression energies that pin
-                          this path (tests/regression_cases.json:99-172) with
-                          the geometries from their .hfinp inputs.
+                          this path (tests/regression_cases.json:99-172), and
+                          its UHF + UMP2 energies of the water radical cation
+                          (tests/regression_cases.json:414-430) and RMP2
+                          energies of water (tests/regression_cases.json:39-50),
+                          with the geometries, charge and multiplicity from
+                          their .hfinp inputs.
   boys_ref.json           Boys-function values produced by the reference's own
                           src/lookup/boys.cpp, compiled unmodified into
                           oracle/_ref/libboys_ref.so (see oracle/build_ref.sh),
@@ -91,10 +95,12 @@ def parse_hfinp(path):
     engine = re.search(r"\bengine\s+(\S+)", text)
     cycles = re.search(r"\bmax_cycles\s+(\d+)", text)
     symm = re.search(r"\buse_symm\s+(\S+)", text)
+    scf_type = re.search(r"\bscf_type\s+(\S+)", text)
     return {"atoms": atoms, "charge": int(m.group(2)), "multiplicity": int(m.group(3)),
             "basis": basis, "engine": engine.group(1) if engine else "os",
             "max_cycles": int(cycles.group(1)) if cycles else 0,
             "use_symm": bool(symm and symm.group(1).lower() == ".true."),
+            "scf_type": scf_type.group(1).lower() if scf_type else "rhf",
             "units": "angstrom"}
 
 
@@ -120,6 +126,7 @@ def main():
         "ethylene_rhf_stability_unstable": "tests/regression_cases.json:144-161",
         "water_rhf_stability_stable": "tests/regression_cases.json:132-143",
         "water_rhf_os_c2v_symmetry_matches_ao_reference": "tests/regression_cases.json:163-172",
+        "water_radical_cation_uhf_ump2_sto3g": "tests/regression_cases.json:414-430",
     }
     out = []
     for case in cases["cases"] if isinstance(cases, dict) else cases:
@@ -130,9 +137,25 @@ def main():
         e = checks["rhf_total_energy"]
         rec = {"id": case["id"], "source": wanted[case["id"]], "input": case["input"],
                "energy": e["expected"], "atol": e["atol"], **inp}
+        if "mp2_total_energy" in checks:
+            rec["mp2_energy"] = checks["mp2_total_energy"]["expected"]
+            rec["mp2_atol"] = checks["mp2_total_energy"]["atol"]
         if "scf_converged_iterations" in checks:
             rec["iterations"] = checks["scf_converged_iterations"]["expected"]
         out.append(rec)
+    # RMP2 pin (tests/regression_cases.json:39-50, water_rmp2_sto3g): its input
+    # inputs/examples/hf/mp2_validation/val_water.hfinp is not in the tree;
+    # its recorded RHF energy equals water_rhf_stability_stable's to all ten
+    # printed digits, so the fixture takes that case's geometry.
+    by_id = {c["id"]: c for c in (cases["cases"] if isinstance(cases, dict) else cases)}
+    base = next(r for r in out if r["id"] == "water_rhf_stability_stable")
+    mp = {c["metric"]: c for c in by_id["water_rmp2_sto3g"]["checks"] if "metric" in c}
+    assert mp["rhf_total_energy"]["expected"] == base["energy"]
+    out.append({**base, "id": "water_rmp2_sto3g", "source": "tests/regression_cases.json:39-50",
+                "input": by_id["water_rmp2_sto3g"]["input"] + " (absent; geometry of water_rhf_stability_stable)",
+                "energy": mp["rhf_total_energy"]["expected"], "atol": mp["rhf_total_energy"]["atol"],
+                "mp2_energy": mp["mp2_total_energy"]["expected"], "mp2_atol": mp["mp2_total_energy"]["atol"]})
+    out[-1].pop("iterations", None)
     with open(os.path.join(HERE, "regression_cases.json"), "w") as f:
         json.dump({"angstrom_to_bohr": 1.8897259886,
                    "angstrom_to_bohr_source": "src/base/tables.h:8",
