@@ -138,6 +138,12 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri);
 pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3,
                             int n3, const double *C4, int n4, double *out);
 
+/* Device time in ms of the last pfk_mo_transform on this context, from CUDA
+ * events on its stream: ms3[0] the AO tensor (clear + class kernels),
+ * ms3[1] the four quarter-transform GEMMs, ms3[2] the copy of the result to
+ * the host.  For measurement. */
+pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3);
+
 /* Per-class work of one build over the 55 classes (ss|ss)..(ff|ff):
  * screened shell quartets, primitive quartets (sum of K_ab * K_cd), and --
  * when ms55 is non-null -- the device time of each class's kernel in a

@@ -33,7 +33,8 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_fock_rhf_noalloc", "pfk_one_electron", "pfk_set_density_screening", "pfk_set_lanes", "pfk_set_primitive_tol", "pfk_autotune", "pfk_mlp_create", "pfk_mlp_destroy", "pfk_mlp_last_error",
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
-           "pfk_checkpoint_last_error", "pfk_mo_transform"]
+           "pfk_checkpoint_last_error", "pfk_mo_transform",
+           "pfk_mo_transform_times"]
 
 _lib = None
 
@@ -85,6 +86,7 @@ def load_library(path=LIB_PATH):
     L.pfk_set_density_screening.argtypes = [vp, c_dbl]
     L.pfk_set_lanes.argtypes = [vp, c_int]
     L.pfk_mo_transform.argtypes = [vp, vp, c_int, vp, c_int, vp, c_int, vp, c_int, vp]
+    L.pfk_mo_transform_times.argtypes = [vp, vp]
     L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
@@ -210,6 +212,12 @@ class FockEngine:
         self._check(self.lib.pfk_mo_transform(self.h, _p(cm[0]), n[0], _p(cm[1]), n[1], _p(cm[2]), n[2],
                                               _p(cm[3]), n[3], _p(out)))
         return out
+
+    def mo_transform_times(self):
+        """(AO tensor, quarter-transform GEMMs, copy-out) device ms of the last mo_transform."""
+        t = np.zeros(3)
+        self._check(self.lib.pfk_mo_transform_times(self.h, _p(t)))
+        return tuple(float(x) for x in t)
 
     def class_stats(self, timed=True):
         """{class name: (shell quartets, primitive quartets, ms)} for non-empty classes."""

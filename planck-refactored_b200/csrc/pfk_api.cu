@@ -70,6 +70,7 @@ struct pfk_ctx {
     cudaStream_t side[kMaxLanes - 1] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes - 1] = {};
     cublasHandle_t blas = nullptr;   // created by the first pfk_mo_transform
+    double mo_ms[3] = {0.0, 0.0, 0.0};   // last pfk_mo_transform: AO tensor, GEMMs, copy out
 
     int nshell = 0, nb = 0;
     std::vector<int> L, bf_off;
@@ -963,10 +964,18 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
         PFK_CK(dC[k].alloc(b * nk[k]));
         PFK_CK(cudaMemcpyAsync(dC[k].p, hC[k], sizeof(double) * b * nk[k], cudaMemcpyHostToDevice, st));
     }
+    cudaEvent_t ev[4] = {};
+    struct EvFree {
+        cudaEvent_t *e;
+        ~EvFree() { for (int k = 0; k < 4; ++k) if (e[k]) cudaEventDestroy(e[k]); }
+    } ev_free{ev};
+    for (auto &x : ev) PFK_CK(cudaEventCreate(&x));
     PFK_CK(E.alloc(b2 * b2));
+    PFK_CK(cudaEventRecord(ev[0], st));
     PFK_CK(cudaMemsetAsync(E.p, 0, sizeof(double) * b2 * b2, st));
     pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, E.p, st, false);
     if (s != PFK_OK) return s;
+    PFK_CK(cudaEventRecord(ev[1], st));
     const double one = 1.0, zero = 0.0;
     auto ck = [&](cublasStatus_t r, const char *what) {
         return r == CUBLAS_STATUS_SUCCESS ? PFK_OK : ctx->fail(PFK_ERR_CUDA, std::string(what) + " failed");
@@ -995,8 +1004,22 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
                        O.p, n4),
            "quarter transform 4 (cublasDgemm)");
     if (s != PFK_OK) return s;
+    PFK_CK(cudaEventRecord(ev[2], st));
     PFK_CK(cudaMemcpyAsync(out, O.p, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
+    PFK_CK(cudaEventRecord(ev[3], st));
     PFK_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 3; ++k) {
+        float ms = 0.f;
+        PFK_CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        ctx->mo_ms[k] = ms;
+    }
+    return PFK_OK;
+}
+
+pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3)
+{
+    if (!ctx || !ms3) return PFK_ERR_STATE;
+    for (int k = 0; k < 3; ++k) ms3[k] = ctx->mo_ms[k];
     return PFK_OK;
 }
 
