@@ -957,7 +957,10 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
     }
     if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return ctx->fail(PFK_ERR_CUDA, "cublasSetStream failed");
     const size_t b = nb, b2 = b * b, b3 = b2 * b;
-    DevBuf<double> E, T1, T2, T3, O, dC[4];
+    // two buffers, allocated before the timed work: the AO tensor E and T1;
+    // T2 (n1 n2 nb^2 <= nb^4) then reuses E, T3 (n1 n2 n3 nb <= n1 nb^3)
+    // reuses T1, and the result (n1 n2 n3 n4 <= n1 n2 nb^2) reuses E
+    DevBuf<double> E, T1, dC[4];
     const double *hC[4] = {C1, C2, C3, C4};
     const int nk[4] = {n1, n2, n3, n4};
     for (int k = 0; k < 4; ++k) {
@@ -971,6 +974,7 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
     } ev_free{ev};
     for (auto &x : ev) PFK_CK(cudaEventCreate(&x));
     PFK_CK(E.alloc(b2 * b2));
+    PFK_CK(T1.alloc(b3 * n1));
     PFK_CK(cudaEventRecord(ev[0], st));
     PFK_CK(cudaMemsetAsync(E.p, 0, sizeof(double) * b2 * b2, st));
     pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, E.p, st, false);
@@ -980,32 +984,26 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
     auto ck = [&](cublasStatus_t r, const char *what) {
         return r == CUBLAS_STATUS_SUCCESS ? PFK_OK : ctx->fail(PFK_ERR_CUDA, std::string(what) + " failed");
     };
-    PFK_CK(T1.alloc(b3 * n1));
+    double *T2 = E.p, *T3 = T1.p, *O = E.p;
     s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)b3, n1, nb, &one, E.p, (int)b3, dC[0].p, nb, &zero,
                        T1.p, (int)b3),
            "quarter transform 1 (cublasDgemm)");
     if (s != PFK_OK) return s;
-    E.release();
-    PFK_CK(T2.alloc(b2 * n1 * n2));
     s = ck(cublasDgemmStridedBatched(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)b2, n2, nb, &one, T1.p, (int)b2,
-                                     (long long)b3, dC[1].p, nb, 0, &zero, T2.p, (int)b2, (long long)b2 * n2, n1),
+                                     (long long)b3, dC[1].p, nb, 0, &zero, T2, (int)b2, (long long)b2 * n2, n1),
            "quarter transform 2 (cublasDgemmStridedBatched)");
     if (s != PFK_OK) return s;
-    T1.release();
-    PFK_CK(T3.alloc(b * n1 * n2 * n3));
-    s = ck(cublasDgemmStridedBatched(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, n3, nb, &one, T2.p, nb, (long long)b2,
-                                     dC[2].p, nb, 0, &zero, T3.p, nb, (long long)b * n3, n1 * n2),
+    s = ck(cublasDgemmStridedBatched(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, n3, nb, &one, T2, nb, (long long)b2,
+                                     dC[2].p, nb, 0, &zero, T3, nb, (long long)b * n3, n1 * n2),
            "quarter transform 3 (cublasDgemmStridedBatched)");
     if (s != PFK_OK) return s;
-    T2.release();
     const size_t no = (size_t)n1 * n2 * n3 * n4;
-    PFK_CK(O.alloc(no));
-    s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, n4, n1 * n2 * n3, nb, &one, dC[3].p, nb, T3.p, nb, &zero,
-                       O.p, n4),
+    s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, n4, n1 * n2 * n3, nb, &one, dC[3].p, nb, T3, nb, &zero,
+                       O, n4),
            "quarter transform 4 (cublasDgemm)");
     if (s != PFK_OK) return s;
     PFK_CK(cudaEventRecord(ev[2], st));
-    PFK_CK(cudaMemcpyAsync(out, O.p, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
+    PFK_CK(cudaMemcpyAsync(out, O, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
     PFK_CK(cudaEventRecord(ev[3], st));
     PFK_CK(cudaStreamSynchronize(st));
     for (int k = 0; k < 3; ++k) {
