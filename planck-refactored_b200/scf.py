@@ -19,9 +19,9 @@ diagonalisation.  Options beyond the reference:
     difference-density build in FP32 (a second context whose whole quartet
     list is on the FP32 path, with density screening at 1e-12: quartets
     whose Schwarz bound times the largest difference-density block they
-    touch is below it are skipped) once the density steps are small, a full
-    FP64 build at least every `full_every` iterations, and one for the final
-    energy;
+    touch is below it are skipped) while the density steps are small but not
+    yet near convergence (max|dP| between 1e-8 and 1e-4), a full FP64 build
+    at least every `full_every` iterations, and one for the final energy;
   * the learned-guess hook (guess.py) supplies P0 and the acceptance rule.
 """
 import numpy as np
@@ -99,16 +99,20 @@ def first_energy(H, enuc, P, G):
 
 
 def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8,
-        incremental=None, full_every=8, incremental_below=1e-4):
+        incremental=None, full_every=8, incremental_below=1e-4, incremental_floor=1e-8):
     """Run RHF to convergence.  engine: FockEngine (its fock_rhf gives
     G = J - K/2).  P0: starting density (default: the core-Hamiltonian
     guess); G0: G(P0) if the caller already built it (the guess hook does).
     incremental: an optional second FockEngine on the same basis set to
     mixed precision with an fp32_bound above every Schwarz bound, used for
-    the difference-density builds once max|P - P_built| < incremental_below
+    the difference-density builds while incremental_floor <= max|P - P_built|
+    < incremental_below
     (an FP32 build of a large difference would carry ~1e-7 relative errors
     into every later G until the next full build), with a full build at
-    least every full_every iterations.  Returns a dict with energy,
+    least every full_every iterations.  Below incremental_floor the steps are
+    within reach of the 1e-10 tests, and the quartets the difference builds
+    screen out (each under 1e-12) add up to errors of that order, so those
+    last iterations use full builds.  Returns a dict with energy,
     iterations, converged, P, C, eps, history and the first-iteration
     energy."""
     nb = H.shape[0]
@@ -122,7 +126,7 @@ def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, 
             G = np.array(G0, dtype=np.float64)
             since_full = 0
         elif (incremental is not None and G is not None and since_full + 1 < full_every
-              and float(np.abs(P - P_built).max()) < incremental_below):
+              and incremental_floor <= float(np.abs(P - P_built).max()) < incremental_below):
             G = G + incremental.fock_rhf(P - P_built)
             since_full += 1
         else:
