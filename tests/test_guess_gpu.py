@@ -70,9 +70,10 @@ def test_shipped_model_reduces_iterations():
 def test_learned_guess_through_a_checkpoint_file(tmp_path):
     """The hook's density written as a .hfchk (checkpoint.save_guess) and
     read back as the reference's `guess density` restart reads it: the
-    density comes back bit for bit, and the SCF started from the file takes
-    the same iterations to the same energy as the SCF started from the hook
-    directly.  A converged SCF written and restarted converges at once."""
+    density comes back bit for bit, and the SCF started from the file
+    reaches the same energy in the same number of iterations (give or take
+    one) as the SCF started from the hook directly.  A converged SCF written
+    and restarted converges at once."""
     P = pfk()
     T = _trainer()
     model = P.guess.GuessModel.load(MODEL)
@@ -87,7 +88,9 @@ def test_learned_guess_through_a_checkpoint_file(tmp_path):
     r_hook = sysm.run(P0=P0)
     r_file = sysm.run(P0=Pf)
     assert r_hook["converged"] and r_file["converged"]
-    assert r_file["iterations"] == r_hook["iterations"]
+    # the builds add in a varying order (FP64 atomics), so the iteration that
+    # first meets the 1e-10 tests can move by one between two identical starts
+    assert abs(r_file["iterations"] - r_hook["iterations"]) <= 1
     assert abs(r_file["energy"] - r_hook["energy"]) < 1e-10
     conv = os.path.join(tmp_path, "converged.hfchk")
     P.checkpoint.write(conv, sysm, r_file["P"], energy=r_file["energy"], converged=True)
