@@ -144,6 +144,16 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
  * the host.  For measurement. */
 pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3);
 
+/* RMP2 correlation energy of a converged RHF (run_rmp2,
+ * src/post_hf/mp2.cpp:10-38, with the amplitudes of mp2_gradient.cpp:203-232):
+ *   E = sum_{iajb} (ia|jb) [2 (ia|jb) - (ib|ja)] / (e_i + e_j - e_a - e_b).
+ * C: host nbasis x nbasis MO coefficients, column-major, the nocc occupied
+ * orbitals first; eps: their nbasis orbital energies.  The (ov|ov) block is
+ * made as by pfk_mo_transform and summed on the device, so it never crosses
+ * to the host; pfk_mo_transform_times then reports the sum as its third
+ * phase.  nbasis <= 180. */
+pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int nocc, double *e_corr);
+
 /* Per-class work of one build over the 55 classes (ss|ss)..(ff|ff):
  * screened shell quartets, primitive quartets (sum of K_ab * K_cd), and --
  * when ms55 is non-null -- the device time of each class's kernel in a

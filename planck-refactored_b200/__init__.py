@@ -34,7 +34,7 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
            "pfk_checkpoint_last_error", "pfk_mo_transform",
-           "pfk_mo_transform_times"]
+           "pfk_mo_transform_times", "pfk_rmp2_energy"]
 
 _lib = None
 
@@ -87,6 +87,7 @@ def load_library(path=LIB_PATH):
     L.pfk_set_lanes.argtypes = [vp, c_int]
     L.pfk_mo_transform.argtypes = [vp, vp, c_int, vp, c_int, vp, c_int, vp, c_int, vp]
     L.pfk_mo_transform_times.argtypes = [vp, vp]
+    L.pfk_rmp2_energy.argtypes = [vp, vp, vp, c_int, ctypes.POINTER(c_dbl)]
     L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
@@ -212,6 +213,15 @@ class FockEngine:
         self._check(self.lib.pfk_mo_transform(self.h, _p(cm[0]), n[0], _p(cm[1]), n[1], _p(cm[2]), n[2],
                                               _p(cm[3]), n[3], _p(out)))
         return out
+
+    def rmp2_energy(self, C, eps, nocc):
+        """RMP2 correlation energy with the (ov|ov) block kept on the device
+        (pfk_rmp2_energy).  C: nbasis x nbasis MO coefficients, occupied first."""
+        cm = np.ascontiguousarray(np.asarray(C, dtype=np.float64).T)   # column-major storage
+        e = _f64(np.asarray(eps, dtype=np.float64).reshape(-1))
+        out = ctypes.c_double(0.0)
+        self._check(self.lib.pfk_rmp2_energy(self.h, _p(cm), _p(e), int(nocc), ctypes.byref(out)))
+        return out.value
 
     def mo_transform_times(self):
         """(AO tensor, quarter-transform GEMMs, copy-out) device ms of the last mo_transform."""

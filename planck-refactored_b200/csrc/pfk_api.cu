@@ -941,11 +941,43 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
 //   T2[i][a][ls] = sum_n C2(n,a) T1[i][n][ls] n1 GEMMs, (nb^2 x nb)(nb x n2)
 //   T3[ia][j][s] = sum_l C3(l,j) T2[ia][l][s] n1 n2 GEMMs, (nb x nb)(nb x n3)
 //   out[iaj][b]  = sum_s T3[iaj][s] C4(s,b)  one GEMM, (n4 x nb)(nb x n1 n2 n3)
-pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3,
-                            int n3, const double *C4, int n4, double *out)
+// RMP2 sum over the (ov|ov) block O[i][a][j][b] in device memory (run_rmp2,
+// src/post_hf/mp2.cpp:25-35, amplitudes mp2_gradient.cpp:216-230):
+//   E += O_iajb (2 O_iajb - O_ibja) / (e_i + e_j - e_a - e_b)
+// Grid-stride over the block, a warp-shuffle and shared-memory reduction per
+// block, one FP64 atomic per block into *out (zeroed by the caller).
+__global__ void __launch_bounds__(256) rmp2_sum_kernel(const double *__restrict__ O, const double *__restrict__ eps,
+                                                       int no, int nv, double *out)
 {
-    if (!ctx) return PFK_ERR_STATE;
-    if (!C1 || !C2 || !C3 || !C4 || !out) return ctx->fail(PFK_ERR_INVALID, "null argument");
+    const long long n = (long long)no * nv * no * nv;
+    double sum = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t % nv);
+        const long long r = t / nv;
+        const int j = (int)(r % no);
+        const long long r2 = r / no;
+        const int a = (int)(r2 % nv), i = (int)(r2 / nv);
+        const double v = O[t];
+        const double w = O[(((long long)i * nv + b) * no + j) * nv + a];
+        sum += v * (2.0 * v - w) / (eps[i] + eps[j] - eps[no + a] - eps[no + b]);
+    }
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    __shared__ double part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += part[w];
+        atomicAdd(out, tot);
+    }
+}
+
+// The transform behind pfk_mo_transform and pfk_rmp2_energy: the result
+// goes to the host buffer `out`, or, with eps set (blocks occ, vir, occ,
+// vir), into the RMP2 sum *e_corr without leaving the device.
+static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3, int n3,
+                         const double *C4, int n4, double *out, const double *eps, double *e_corr)
+{
     const int nb = ctx->nb;
     if (n1 < 1 || n2 < 1 || n3 < 1 || n4 < 1 || n1 > nb || n2 > nb || n3 > nb || n4 > nb)
         return ctx->fail(PFK_ERR_INVALID, "need 1 <= n_k <= nbasis");
@@ -1003,8 +1035,21 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
            "quarter transform 4 (cublasDgemm)");
     if (s != PFK_OK) return s;
     PFK_CK(cudaEventRecord(ev[2], st));
-    PFK_CK(cudaMemcpyAsync(out, O, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
-    PFK_CK(cudaEventRecord(ev[3], st));
+    if (eps) {
+        DevBuf<double> d_eps, d_sum;
+        PFK_CK(d_eps.alloc(nb));
+        PFK_CK(d_sum.alloc(1));
+        PFK_CK(cudaMemcpyAsync(d_eps.p, eps, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+        PFK_CK(cudaMemsetAsync(d_sum.p, 0, sizeof(double), st));
+        rmp2_sum_kernel<<<148 * 8, 256, 0, st>>>(O, d_eps.p, n1, n2, d_sum.p);
+        PFK_CK(cudaGetLastError());
+        PFK_CK(cudaMemcpyAsync(e_corr, d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        PFK_CK(cudaEventRecord(ev[3], st));
+        PFK_CK(cudaStreamSynchronize(st));
+    } else {
+        PFK_CK(cudaMemcpyAsync(out, O, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
+        PFK_CK(cudaEventRecord(ev[3], st));
+    }
     PFK_CK(cudaStreamSynchronize(st));
     for (int k = 0; k < 3; ++k) {
         float ms = 0.f;
@@ -1012,6 +1057,24 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
         ctx->mo_ms[k] = ms;
     }
     return PFK_OK;
+}
+
+pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3,
+                            int n3, const double *C4, int n4, double *out)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!C1 || !C2 || !C3 || !C4 || !out) return ctx->fail(PFK_ERR_INVALID, "null argument");
+    return mo_run(ctx, C1, n1, C2, n2, C3, n3, C4, n4, out, nullptr, nullptr);
+}
+
+pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int nocc, double *e_corr)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!C || !eps || !e_corr) return ctx->fail(PFK_ERR_INVALID, "null argument");
+    const int nb = ctx->nb, nv = nb - nocc;
+    if (nocc < 1 || nv < 1) return ctx->fail(PFK_ERR_INVALID, "no occupied or virtual orbitals");
+    const double *Cv = C + (size_t)nb * nocc;   // column-major: the virtual columns follow
+    return mo_run(ctx, C, nocc, Cv, nv, C, nocc, Cv, nv, nullptr, eps, e_corr);
 }
 
 pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3)

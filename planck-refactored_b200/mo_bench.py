@@ -9,7 +9,8 @@ Reports, per phase, the device time from CUDA events inside the call: the
 AO tensor (class kernels in tensor mode; 8-fold scatter of every screened
 integral), the four quarter-transform GEMMs (FP64, cuBLAS) with their
 FLOP rate against the FP64 FMA peak measured in the same run, and the copy
-of the MO block to the host; and the RMP2 energy.
+of the MO block to the host; and the RMP2 energy, summed on the host from
+that block and on the device (pfk_rmp2_energy, the block never leaving HBM).
 """
 import argparse
 import json
@@ -44,13 +45,20 @@ def main():
     flops = 2.0 * (no * nb ** 4 + no * nv * nb ** 3 + no * nv * no * nb ** 2 + no * nv * no * nv * nb)
     fp64_peak, _ = P.measure_fma_peak(0)
     e2 = P.mp2.rmp2(eng, C, r["eps"], no)
+    dev = []
+    for _ in range(a.reps):
+        e_dev = eng.rmp2_energy(C, r["eps"], no)
+        dev.append(eng.mo_transform_times())
+    td = min(dev, key=lambda x: x[1])
     sysm.close()
     out = {"workload": f"(H2O){a.waters} 6-31G** ({nb} bf), MP2 block (occ vir|occ vir), nocc {no}, nvir {nv}",
            "ao_tensor_ms": t[0], "ao_tensor_GBps_written": nb ** 4 * 8 / t[0] / 1e6,
            "gemm_ms": t[1], "gemm_flops": flops, "gemm_tflops": flops / t[1] / 1e9,
            "fp64_fma_peak_tflops": fp64_peak, "gemm_frac_of_fp64_peak": flops / t[1] / 1e9 / fp64_peak,
            "copy_out_ms": t[2], "mo_block_MB": no * nv * no * nv * 8 / 1e6,
-           "rhf_energy": r["energy"], "rmp2_corr": e2}
+           "rhf_energy": r["energy"], "rmp2_corr": e2,
+           "rmp2_on_device": {"corr": e_dev, "ao_tensor_ms": td[0], "gemm_ms": td[1], "sum_ms": td[2],
+                              "total_ms": sum(td), "block_read_GBps": 2 * no * nv * no * nv * 8 / td[2] / 1e6}}
     print(json.dumps(out))
 
 

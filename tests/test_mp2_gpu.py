@@ -44,12 +44,14 @@ def test_rmp2_matches_the_oracle_and_ump2():
     C, eps, nocc = r["C"], r["eps"], sysm.nocc
     e_gpu = P.mp2.rmp2(sysm.engine, C, eps, nocc)
     e_u = P.mp2.ump2(sysm.engine, C, eps, C, eps, nocc, nocc)
+    e_dev = sysm.engine.rmp2_energy(C, eps, nocc)   # the sum on the device
     sysm.close()
     eri_o, _ = oracle.Basis(oracle.shells_for(oracle.Molecule(WATER), "6-31g**")).eri_tensor(1e-10, oracle.OS)
     e_o = mo_ref.rmp2_energy(eri_o, C, eps, nocc)
     assert -0.3 < e_gpu < -0.1
     assert abs(e_gpu - e_o) < 1e-10
     assert abs(e_u - e_gpu) < 1e-10
+    assert abs(e_dev - e_gpu) < 1e-12
 
 
 def test_rhf_and_rmp2_match_the_reference_regression():
@@ -61,8 +63,10 @@ def test_rhf_and_rmp2_match_the_reference_regression():
     sysm = P.scf.System(c["atoms"], c["basis"], basis_library())
     r = sysm.run()
     e_corr = P.mp2.rmp2(sysm.engine, r["C"], r["eps"], sysm.nocc)
+    e_dev = sysm.engine.rmp2_energy(r["C"], r["eps"], sysm.nocc)
     sysm.close()
     assert r["converged"]
+    assert abs(r["energy"] + e_dev - c["mp2_energy"]) < c["mp2_atol"]
     assert abs(r["energy"] - c["energy"]) < c["atol"]
     assert abs(r["energy"] + e_corr - c["mp2_energy"]) < c["mp2_atol"]
 
