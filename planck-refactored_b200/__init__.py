@@ -130,6 +130,7 @@ class FockEngine:
             raise PfkError(st, self.lib.pfk_last_error(None).decode())
         self.h = h
         self.nbasis = self.lib.pfk_nbasis(h)
+        self.device = int(device)
         self.tol_eri, self.engine, self.precision, self.fp32_bound = 1e-10, "os", "fp64", fp32_bound
         self.set_options(tol_eri, engine, precision, fp32_bound)
 

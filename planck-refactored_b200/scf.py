@@ -154,6 +154,79 @@ def rhf(engine, H, S, enuc, nocc, P0=None, G0=None, max_iter=None, tol_e=1e-10, 
             "history": history, "first_energy": E_first}
 
 
+def rhf_device(engine, H, S, enuc, nocc, P0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8):
+    """The loop of rhf() with its linear algebra on the GPU: the density stays
+    in HBM and feeds pfk_fock_rhf_device (one captured graph, replayed every
+    iteration), and F, the DIIS errors and products, the diagonalisation
+    (torch.linalg.eigh: cuSOLVER) and the convergence tests run there in
+    FP64; only the DIIS system (at most 9 x 9) is solved on the host, with the
+    same pivoted QR.  Not in the reference, which keeps this on the host; the
+    steps are rhf()'s, so it converges to the same energy, though the
+    eigensolver's rounding can move the iteration that first meets the 1e-10
+    tests.  Returns rhf()'s dict (numpy arrays) plus build_seconds, the device
+    time of the Fock builds."""
+    import torch
+    dev = torch.device("cuda", getattr(engine, "device", 0))
+    f64 = dict(dtype=torch.float64, device=dev)
+    nb = H.shape[0]
+    Ht, St = torch.tensor(H, **f64), torch.tensor(S, **f64)
+    X = torch.tensor(orthogonaliser(S), **f64)
+    P = torch.tensor(hcore_density(H, orthogonaliser(S), nocc) if P0 is None else P0, **f64)
+    dP, dG = torch.empty_like(P), torch.empty_like(P)
+    # one non-default stream for torch's work and the build, so that they are
+    # ordered (a null handle would send the build to the context's own stream)
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        return _rhf_device_loop(engine, Ht, St, X, P, dP, dG, stream, enuc, nocc, nb, max_iter, tol_e, tol_d,
+                                diis_depth)
+
+
+def _rhf_device_loop(engine, Ht, St, X, P, dP, dG, stream, enuc, nocc, nb, max_iter, tol_e, tol_d, diis_depth):
+    import torch
+    max_iter = max_iter or max_cycles(nb)
+    Fs, Es = [], []
+    E_prev, history, E_first, build_ms = 0.0, [], None, 0.0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for it in range(1, max_iter + 1):
+        dP.copy_(P)
+        ev[0].record(stream)
+        engine.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), stream.cuda_stream)
+        ev[1].record(stream)
+        F = Ht + dG
+        E = 0.5 * float(torch.sum(P * (Ht + F))) + enuc
+        build_ms += ev[0].elapsed_time(ev[1])
+        if E_first is None:
+            E_first = E
+        err = X.T @ (F @ P @ St - St @ P @ F) @ X
+        Fs, Es = (Fs + [F])[-diis_depth:], (Es + [err])[-diis_depth:]
+        m = len(Fs)
+        if m < 2:
+            Fx = F
+        else:
+            Et = torch.stack([e.reshape(-1) for e in Es])
+            B = -np.ones((m + 1, m + 1))
+            B[m, m] = 0.0
+            B[:m, :m] = (Et @ Et.T).cpu().numpy()
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            c = _lstsq_pivoted(B, rhs)
+            Fx = sum(float(c[i]) * Fs[i] for i in range(m))
+        eps, Cp = torch.linalg.eigh(X.T @ Fx @ X)
+        C = X @ Cp
+        Pn = 2.0 * C[:, :nocc] @ C[:, :nocc].T
+        d = Pn - P
+        dE = abs(E - E_prev)
+        dmax, drms = float(d.abs().max()), float(torch.sqrt(torch.mean(d * d)))
+        history.append((it, E, dE, drms, dmax))
+        P, E_prev = Pn, E
+        if it > 1 and dE < tol_e and drms < tol_d and dmax < tol_d:
+            return {"energy": E, "iterations": it, "converged": True, "P": P.cpu().numpy(), "C": C.cpu().numpy(),
+                    "eps": eps.cpu().numpy(), "history": history, "first_energy": E_first,
+                    "build_seconds": build_ms * 1e-3}
+    return {"energy": E_prev, "iterations": max_iter, "converged": False, "P": P.cpu().numpy(), "C": C.cpu().numpy(),
+            "eps": eps.cpu().numpy(), "history": history, "first_energy": E_first, "build_seconds": build_ms * 1e-3}
+
+
 def uhf(engine, H, S, enuc, n_alpha, n_beta, P0=None, max_iter=None, tol_e=1e-10, tol_d=1e-10, diis_depth=8):
     """UHF to convergence (the loop of run_uhf, src/scf/scf.cpp:467-930) on
     FockEngine.fock_uhf (Ga = J(Pa+Pb) - K(Pa), Gb = J(Pa+Pb) - K(Pb)).
@@ -226,7 +299,14 @@ class System:
             self._incr.set_density_screening(1e-12)
         return self._incr
 
-    def run(self, P0=None, incremental=False, **kw):
+    def run(self, P0=None, incremental=False, linalg="host", **kw):
+        """RHF to convergence; linalg="device" runs rhf_device (the loop's
+        linear algebra on the GPU) instead of rhf."""
+        if linalg == "device":
+            if incremental:
+                raise ValueError("the device loop has no difference-density builds")
+            kw.pop("G0", None)   # the device loop makes its first build itself
+            return rhf_device(self.engine, self.H, self.S, self.enuc, self.nocc, P0=P0, **kw)
         return rhf(self.engine, self.H, self.S, self.enuc, self.nocc, P0=P0,
                    incremental=self.incremental_engine() if incremental else None, **kw)
 

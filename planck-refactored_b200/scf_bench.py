@@ -58,7 +58,7 @@ class _Timed:
         return G
 
 
-def run(name, device=0, guess_model=None, runs=None):
+def run(name, device=0, guess_model=None, runs=None, linalg="host"):
     P = _pkg()
     atoms, basis = molecule(name)
     lib = P.basis.load_library()
@@ -71,6 +71,9 @@ def run(name, device=0, guess_model=None, runs=None):
         plan += [("fp64+guess", "fp64", False, True), ("mixed+guess", "mixed", False, True)]
     if runs:
         plan = [p for p in plan if p[0] in runs]
+    if linalg == "device":   # the device loop has no difference-density builds
+        plan = [p for p in plan if not p[2]]
+    out["linalg"] = linalg
     ref = None
     for label, prec, incr, learned in plan:
         t0 = time.perf_counter()
@@ -83,7 +86,11 @@ def run(name, device=0, guess_model=None, runs=None):
         hook = None
         if learned:
             P0, G0, hook = P.guess.choose(model, sysm)
-        r = P.scf.rhf(full, sysm.H, sysm.S, sysm.enuc, sysm.nocc, P0=P0, G0=G0, incremental=incr_eng)
+        if linalg == "device":
+            r = P.scf.rhf_device(sysm.engine, sysm.H, sysm.S, sysm.enuc, sysm.nocc, P0=P0)
+            full.seconds += r["build_seconds"]
+        else:
+            r = P.scf.rhf(full, sysm.H, sysm.S, sysm.enuc, sysm.nocc, P0=P0, G0=G0, incremental=incr_eng)
         t_scf = time.perf_counter() - t0
         out["nbasis"] = int(sysm.H.shape[0])
         sysm.close()
@@ -113,8 +120,10 @@ def main():
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--guess-model", default=None, help="learned-guess model in the molecule's basis")
     ap.add_argument("--runs", default=None, help="comma-separated subset of fp64,mixed,mixed+dP,fp64+guess,mixed+guess")
+    ap.add_argument("--linalg", default="host", choices=["host", "device"],
+                    help="device: the SCF loop's diagonalisation and DIIS on the GPU (scf.rhf_device)")
     a = ap.parse_args()
-    res = run(a.molecule, a.device, a.guess_model, a.runs.split(",") if a.runs else None)
+    res = run(a.molecule, a.device, a.guess_model, a.runs.split(",") if a.runs else None, a.linalg)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f, indent=1)

@@ -116,3 +116,20 @@ def test_density_screening_of_a_difference_build():
     assert np.abs(G_scr - G_full).max() < 1e-10
     assert not np.any(G_zero)
     assert np.abs(G_again - G_full).max() < 1e-15
+
+
+def test_device_linear_algebra_loop_matches_the_host_loop():
+    """scf.rhf_device (density in HBM, eigh and DIIS on the GPU) converges to
+    the host loop's energy (1e-9 Eh) within a couple of iterations of it, from
+    the default guess and from a supplied density."""
+    P = pfk()
+    sysm = P.scf.System(water_cluster(3, seed=5), "6-31g**", basis_library())
+    r_h = sysm.run()
+    r_d = sysm.run(linalg="device")
+    r_d2 = sysm.run(P0=r_h["P"], linalg="device")
+    sysm.close()
+    assert r_h["converged"] and r_d["converged"] and r_d2["converged"]
+    assert abs(r_d["energy"] - r_h["energy"]) < 1e-9
+    assert abs(r_d["iterations"] - r_h["iterations"]) <= 2
+    assert r_d2["iterations"] <= 3 and abs(r_d2["energy"] - r_h["energy"]) < 1e-9
+    assert r_d["build_seconds"] > 0
