@@ -154,6 +154,16 @@ pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3);
  * phase.  nbasis <= 180. */
 pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int nocc, double *e_corr);
 
+/* UMP2 correlation energy of a converged UHF (run_ump2,
+ * src/post_hf/mp2.cpp:43-143): the alpha-alpha and beta-beta terms
+ * 1/4 sum [(ia|jb) - (ib|ja)]^2 / D and the alpha-beta term sum (ia|jb)^2 / D
+ * over three device-resident (ov|ov) blocks, each made as by
+ * pfk_mo_transform and summed where it was made.  Ca, Cb: host nbasis x
+ * nbasis MO coefficients per spin, column-major, occupied first; eps_a, eps_b
+ * their orbital energies.  nbasis <= 180. */
+pfk_status pfk_ump2_energy(pfk_ctx *ctx, const double *Ca, const double *eps_a, const double *Cb, const double *eps_b,
+                           int n_alpha, int n_beta, double *e_corr);
+
 /* Per-class work of one build over the 55 classes (ss|ss)..(ff|ff):
  * screened shell quartets, primitive quartets (sum of K_ab * K_cd), and --
  * when ms55 is non-null -- the device time of each class's kernel in a

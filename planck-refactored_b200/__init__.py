@@ -34,7 +34,8 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_mlp_param_count", "pfk_mlp_set_params", "pfk_mlp_get_params", "pfk_mlp_forward", "pfk_mlp_gradients",
            "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
            "pfk_checkpoint_last_error", "pfk_mo_transform",
-           "pfk_mo_transform_times", "pfk_rmp2_energy"]
+           "pfk_mo_transform_times", "pfk_rmp2_energy",
+           "pfk_ump2_energy"]
 
 _lib = None
 
@@ -88,6 +89,7 @@ def load_library(path=LIB_PATH):
     L.pfk_mo_transform.argtypes = [vp, vp, c_int, vp, c_int, vp, c_int, vp, c_int, vp]
     L.pfk_mo_transform_times.argtypes = [vp, vp]
     L.pfk_rmp2_energy.argtypes = [vp, vp, vp, c_int, ctypes.POINTER(c_dbl)]
+    L.pfk_ump2_energy.argtypes = [vp, vp, vp, vp, vp, c_int, c_int, ctypes.POINTER(c_dbl)]
     L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
     _lib = L
@@ -222,6 +224,18 @@ class FockEngine:
         e = _f64(np.asarray(eps, dtype=np.float64).reshape(-1))
         out = ctypes.c_double(0.0)
         self._check(self.lib.pfk_rmp2_energy(self.h, _p(cm), _p(e), int(nocc), ctypes.byref(out)))
+        return out.value
+
+    def ump2_energy(self, Ca, eps_a, Cb, eps_b, n_alpha, n_beta):
+        """UMP2 correlation energy with the three (ov|ov) blocks kept on the
+        device (pfk_ump2_energy).  Ca, Cb: MO coefficients, occupied first."""
+        ca = np.ascontiguousarray(np.asarray(Ca, dtype=np.float64).T)
+        cb = np.ascontiguousarray(np.asarray(Cb, dtype=np.float64).T)
+        ea = _f64(np.asarray(eps_a, dtype=np.float64).reshape(-1))
+        eb = _f64(np.asarray(eps_b, dtype=np.float64).reshape(-1))
+        out = ctypes.c_double(0.0)
+        self._check(self.lib.pfk_ump2_energy(self.h, _p(ca), _p(ea), _p(cb), _p(eb), int(n_alpha), int(n_beta),
+                                             ctypes.byref(out)))
         return out.value
 
     def mo_transform_times(self):

@@ -941,25 +941,37 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
 //   T2[i][a][ls] = sum_n C2(n,a) T1[i][n][ls] n1 GEMMs, (nb^2 x nb)(nb x n2)
 //   T3[ia][j][s] = sum_l C3(l,j) T2[ia][l][s] n1 n2 GEMMs, (nb x nb)(nb x n3)
 //   out[iaj][b]  = sum_s T3[iaj][s] C4(s,b)  one GEMM, (n4 x nb)(nb x n1 n2 n3)
-// RMP2 sum over the (ov|ov) block O[i][a][j][b] in device memory (run_rmp2,
-// src/post_hf/mp2.cpp:25-35, amplitudes mp2_gradient.cpp:216-230):
-//   E += O_iajb (2 O_iajb - O_ibja) / (e_i + e_j - e_a - e_b)
-// Grid-stride over the block, a warp-shuffle and shared-memory reduction per
-// block, one FP64 atomic per block into *out (zeroed by the caller).
-__global__ void __launch_bounds__(256) rmp2_sum_kernel(const double *__restrict__ O, const double *__restrict__ eps,
-                                                       int no, int nv, double *out)
+// MP2 sums over an (ov|ov) block O[i][a][j][b] (dimensions n1 n2 n3 n4) in
+// device memory, with D = e1_i + e2_j - e1_{n1+a} - e2_{n3+b} (e1 and e2 the
+// orbital energies of the two spins, occupied first):
+//   kMp2R    O (2 O - O_ibja) / D       RMP2 (run_rmp2, src/post_hf/mp2.cpp:
+//                                       25-35; mp2_gradient.cpp:216-230)
+//   kMp2Same (O - O_ibja)^2 / (4 D)     UMP2 same spin (mp2.cpp:93-124)
+//   kMp2Opp  O^2 / D                    UMP2 opposite spin (mp2.cpp:126-139)
+// O_ibja needs n1 = n3 and n2 = n4.  Grid-stride over the block, a
+// warp-shuffle and shared-memory reduction per block, one FP64 atomic per
+// block into *out (zeroed by the caller).
+constexpr int kMp2R = 0, kMp2Same = 1, kMp2Opp = 2;
+__global__ void __launch_bounds__(256) mp2_sum_kernel(const double *__restrict__ O, const double *__restrict__ e1,
+                                                      const double *__restrict__ e2, int n1, int n2, int n3, int n4,
+                                                      int mode, double *out)
 {
-    const long long n = (long long)no * nv * no * nv;
+    const long long n = (long long)n1 * n2 * n3 * n4;
     double sum = 0.0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int b = (int)(t % nv);
-        const long long r = t / nv;
-        const int j = (int)(r % no);
-        const long long r2 = r / no;
-        const int a = (int)(r2 % nv), i = (int)(r2 / nv);
+        const int b = (int)(t % n4);
+        const long long r = t / n4;
+        const int j = (int)(r % n3);
+        const long long r2 = r / n3;
+        const int a = (int)(r2 % n2), i = (int)(r2 / n2);
         const double v = O[t];
-        const double w = O[(((long long)i * nv + b) * no + j) * nv + a];
-        sum += v * (2.0 * v - w) / (eps[i] + eps[j] - eps[no + a] - eps[no + b]);
+        const double D = e1[i] + e2[j] - e1[n1 + a] - e2[n3 + b];
+        if (mode == kMp2Opp) {
+            sum += v * v / D;
+        } else {
+            const double w = O[(((long long)i * n2 + b) * n3 + j) * n4 + a];
+            sum += mode == kMp2R ? v * (2.0 * v - w) / D : 0.25 * (v - w) * (v - w) / D;
+        }
     }
     for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     __shared__ double part[8];
@@ -972,11 +984,14 @@ __global__ void __launch_bounds__(256) rmp2_sum_kernel(const double *__restrict_
     }
 }
 
-// The transform behind pfk_mo_transform and pfk_rmp2_energy: the result
-// goes to the host buffer `out`, or, with eps set (blocks occ, vir, occ,
-// vir), into the RMP2 sum *e_corr without leaving the device.
+// The transform behind pfk_mo_transform and the MP2 entry points: the
+// result goes to the host buffer `out`, or, with eps1 set (blocks occ, vir,
+// occ, vir; eps1 and eps2 the nbasis orbital energies of the first and the
+// second pair's spin), into the MP2 sum of `mode` in *e_corr without leaving
+// the device.
 static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3, int n3,
-                         const double *C4, int n4, double *out, const double *eps, double *e_corr)
+                         const double *C4, int n4, double *out, const double *eps1, const double *eps2, int mode,
+                         double *e_corr)
 {
     const int nb = ctx->nb;
     if (n1 < 1 || n2 < 1 || n3 < 1 || n4 < 1 || n1 > nb || n2 > nb || n3 > nb || n4 > nb)
@@ -1035,13 +1050,14 @@ static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C
            "quarter transform 4 (cublasDgemm)");
     if (s != PFK_OK) return s;
     PFK_CK(cudaEventRecord(ev[2], st));
-    if (eps) {
+    if (eps1) {
         DevBuf<double> d_eps, d_sum;
-        PFK_CK(d_eps.alloc(nb));
+        PFK_CK(d_eps.alloc(2 * b));
         PFK_CK(d_sum.alloc(1));
-        PFK_CK(cudaMemcpyAsync(d_eps.p, eps, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+        PFK_CK(cudaMemcpyAsync(d_eps.p, eps1, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+        PFK_CK(cudaMemcpyAsync(d_eps.p + nb, eps2, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
         PFK_CK(cudaMemsetAsync(d_sum.p, 0, sizeof(double), st));
-        rmp2_sum_kernel<<<148 * 8, 256, 0, st>>>(O, d_eps.p, n1, n2, d_sum.p);
+        mp2_sum_kernel<<<148 * 8, 256, 0, st>>>(O, d_eps.p, d_eps.p + nb, n1, n2, n3, n4, mode, d_sum.p);
         PFK_CK(cudaGetLastError());
         PFK_CK(cudaMemcpyAsync(e_corr, d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         PFK_CK(cudaEventRecord(ev[3], st));
@@ -1064,7 +1080,7 @@ pfk_status pfk_mo_transform(pfk_ctx *ctx, const double *C1, int n1, const double
 {
     if (!ctx) return PFK_ERR_STATE;
     if (!C1 || !C2 || !C3 || !C4 || !out) return ctx->fail(PFK_ERR_INVALID, "null argument");
-    return mo_run(ctx, C1, n1, C2, n2, C3, n3, C4, n4, out, nullptr, nullptr);
+    return mo_run(ctx, C1, n1, C2, n2, C3, n3, C4, n4, out, nullptr, nullptr, 0, nullptr);
 }
 
 pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int nocc, double *e_corr)
@@ -1074,7 +1090,26 @@ pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int
     const int nb = ctx->nb, nv = nb - nocc;
     if (nocc < 1 || nv < 1) return ctx->fail(PFK_ERR_INVALID, "no occupied or virtual orbitals");
     const double *Cv = C + (size_t)nb * nocc;   // column-major: the virtual columns follow
-    return mo_run(ctx, C, nocc, Cv, nv, C, nocc, Cv, nv, nullptr, eps, e_corr);
+    return mo_run(ctx, C, nocc, Cv, nv, C, nocc, Cv, nv, nullptr, eps, eps, kMp2R, e_corr);
+}
+
+pfk_status pfk_ump2_energy(pfk_ctx *ctx, const double *Ca, const double *eps_a, const double *Cb, const double *eps_b,
+                           int n_alpha, int n_beta, double *e_corr)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!Ca || !eps_a || !Cb || !eps_b || !e_corr) return ctx->fail(PFK_ERR_INVALID, "null argument");
+    const int nb = ctx->nb, nva = nb - n_alpha, nvb = nb - n_beta;
+    if (n_alpha < 1 || nva < 1 || n_beta < 1 || nvb < 1)
+        return ctx->fail(PFK_ERR_INVALID, "no occupied or virtual orbitals in a spin channel");
+    const double *Cav = Ca + (size_t)nb * n_alpha, *Cbv = Cb + (size_t)nb * n_beta;
+    double e_aa = 0.0, e_bb = 0.0, e_ab = 0.0;
+    pfk_status s = mo_run(ctx, Ca, n_alpha, Cav, nva, Ca, n_alpha, Cav, nva, nullptr, eps_a, eps_a, kMp2Same, &e_aa);
+    if (s == PFK_OK)
+        s = mo_run(ctx, Cb, n_beta, Cbv, nvb, Cb, n_beta, Cbv, nvb, nullptr, eps_b, eps_b, kMp2Same, &e_bb);
+    if (s == PFK_OK)
+        s = mo_run(ctx, Ca, n_alpha, Cav, nva, Cb, n_beta, Cbv, nvb, nullptr, eps_a, eps_b, kMp2Opp, &e_ab);
+    if (s == PFK_OK) *e_corr = e_aa + e_bb + e_ab;
+    return s;
 }
 
 pfk_status pfk_mo_transform_times(const pfk_ctx *ctx, double *ms3)

@@ -45,6 +45,7 @@ def test_rmp2_matches_the_oracle_and_ump2():
     e_gpu = P.mp2.rmp2(sysm.engine, C, eps, nocc)
     e_u = P.mp2.ump2(sysm.engine, C, eps, C, eps, nocc, nocc)
     e_dev = sysm.engine.rmp2_energy(C, eps, nocc)   # the sum on the device
+    e_udev = sysm.engine.ump2_energy(C, eps, C, eps, nocc, nocc)
     sysm.close()
     eri_o, _ = oracle.Basis(oracle.shells_for(oracle.Molecule(WATER), "6-31g**")).eri_tensor(1e-10, oracle.OS)
     e_o = mo_ref.rmp2_energy(eri_o, C, eps, nocc)
@@ -52,6 +53,7 @@ def test_rmp2_matches_the_oracle_and_ump2():
     assert abs(e_gpu - e_o) < 1e-10
     assert abs(e_u - e_gpu) < 1e-10
     assert abs(e_dev - e_gpu) < 1e-12
+    assert abs(e_udev - e_gpu) < 1e-10
 
 
 def test_rhf_and_rmp2_match_the_reference_regression():
@@ -99,6 +101,7 @@ def test_uhf_and_ump2_of_the_water_cation():
     na, nb_ = (nelec + c["multiplicity"] - 1) // 2, (nelec - c["multiplicity"] + 1) // 2
     r = P.scf.uhf(sysm.engine, sysm.H, sysm.S, sysm.enuc, na, nb_)
     e_corr = P.mp2.ump2(sysm.engine, r["Ca"], r["eps_a"], r["Cb"], r["eps_b"], na, nb_)
+    e_dev = sysm.engine.ump2_energy(r["Ca"], r["eps_a"], r["Cb"], r["eps_b"], na, nb_)   # sums on the device
     H, S, enuc = sysm.H, sysm.S, sysm.enuc
     sysm.close()
     mol = oracle.Molecule(c["atoms"], charge=c["charge"])
@@ -108,5 +111,6 @@ def test_uhf_and_ump2_of_the_water_cation():
     assert r["converged"] and r_o["converged"]
     assert abs(r["energy"] - r_o["energy"]) < 1e-10
     assert abs(e_corr - e_corr_o) < 1e-10
+    assert abs(e_dev - e_corr) < 1e-12
     assert abs(r["energy"] - c["energy"]) < 1e-8
     assert abs(r["energy"] + e_corr - c["mp2_energy"]) < 1e-6
