@@ -71,6 +71,9 @@ struct pfk_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes - 1] = {};
     cublasHandle_t blas = nullptr;   // created by the first pfk_mo_transform
     double mo_ms[3] = {0.0, 0.0, 0.0};   // last pfk_mo_transform: AO tensor, GEMMs, copy out
+    // two pinned staging chunks for copying MO blocks into pageable host memory
+    void *pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 
     int nshell = 0, nb = 0;
     std::vector<int> L, bf_off;
@@ -731,6 +734,10 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
     }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->blas) cublasDestroy(ctx->blas);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->pin[k]) cudaFreeHost(ctx->pin[k]);
+        if (ctx->pin_ev[k]) cudaEventDestroy(ctx->pin_ev[k]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PFK_OK;
@@ -1063,8 +1070,36 @@ static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C
         PFK_CK(cudaEventRecord(ev[3], st));
         PFK_CK(cudaStreamSynchronize(st));
     } else {
-        PFK_CK(cudaMemcpyAsync(out, O, sizeof(double) * no, cudaMemcpyDeviceToHost, st));
+        // the caller's buffer is pageable: stage it through two pinned chunks,
+        // so the device copy runs at pinned speed and the host copy of one
+        // chunk overlaps the device copy of the next
+        constexpr size_t kChunk = size_t(16) << 20;   // bytes per chunk
+        for (int k = 0; k < 2; ++k) {
+            if (!ctx->pin[k]) PFK_CK(cudaHostAlloc(&ctx->pin[k], kChunk, cudaHostAllocDefault));
+            if (!ctx->pin_ev[k]) PFK_CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
+        }
+        const size_t bytes = sizeof(double) * no;
+        const char *src = reinterpret_cast<const char *>(O);
+        char *dst = reinterpret_cast<char *>(out);
+        size_t prev_off = 0, prev_n = 0;
+        int k = 0;
+        for (size_t off = 0; off < bytes; off += kChunk, ++k) {
+            const int bi = k & 1;
+            const size_t n = std::min(kChunk, bytes - off);
+            PFK_CK(cudaMemcpyAsync(ctx->pin[bi], src + off, n, cudaMemcpyDeviceToHost, st));
+            PFK_CK(cudaEventRecord(ctx->pin_ev[bi], st));
+            if (k > 0) {   // the previous chunk, in the other buffer
+                PFK_CK(cudaEventSynchronize(ctx->pin_ev[1 - bi]));
+                std::memcpy(dst + prev_off, ctx->pin[1 - bi], prev_n);
+            }
+            prev_off = off;
+            prev_n = n;
+        }
         PFK_CK(cudaEventRecord(ev[3], st));
+        if (k > 0) {
+            PFK_CK(cudaEventSynchronize(ctx->pin_ev[(k - 1) & 1]));
+            std::memcpy(dst + prev_off, ctx->pin[(k - 1) & 1], prev_n);
+        }
     }
     PFK_CK(cudaStreamSynchronize(st));
     for (int k = 0; k < 3; ++k) {
