@@ -195,6 +195,72 @@ def _traffic_from_profiles(kernel_class):
         return None
 
 
+def time_to_energy(device, runs=("fp64", "mixed+guess", "mixed+guess+dP"), model_path=None):
+    """Time to the converged RHF energy of C40H82 / cc-pVDZ (1010 Cartesian
+    functions; all-trans, seeded +-0.03 Angstrom noise), each arm a fresh
+    context and a whole SCF through the C ABI (pfk_scf_rhf: builds, DIIS and
+    diagonalisation on the device), wall-clocked from the start of the guess
+    to the converged energy:
+      fp64            the plain all-FP64 GPU path, core-Hamiltonian guess;
+      mixed+guess     FP32 below a Schwarz bound of 1e-8, learned guess;
+      mixed+guess+dP  the same with FP32 difference-density builds.
+    Setup (pair data, Schwarz table, lists, one-electron integrals) is timed
+    separately and is the same for every arm."""
+    P = _pfk()
+    atoms = P.workloads.alkane(40, seed=3, noise=0.03)
+    lib = P.basis.load_library()
+    model_path = model_path or os.path.join(REPO, "planck-refactored_b200", "data", "guess_model_ccpvdz.npz")
+    model = P.guess.GuessModel.load(model_path, device=device)
+    out = {"molecule": "C40H82 cc-pVDZ (1010 Cartesian functions), seed 3", "arms": {}}
+    ref = None
+    for label in runs:
+        prec = "fp64" if label == "fp64" else "mixed"
+        t0 = time.perf_counter()
+        sysm = P.scf.System(atoms, "cc-pvdz", lib, device=device, precision=prec, fp32_bound=1e-8)
+        if "dP" in label:
+            sysm.incremental_engine()
+        t_setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        P0 = G0 = None
+        hook = None
+        if "guess" in label:
+            P0, G0, hook = P.guess.choose(model, sysm)
+        t_guess = time.perf_counter() - t0
+        r = sysm.run(P0=P0, G0=G0, linalg="gpu", incremental="dP" in label)
+        wall = time.perf_counter() - t0
+        sysm.close()
+        if ref is None:
+            ref = r["energy"]
+        # the first iteration from which the energy stays within 1e-6 Eh of
+        # the converged one, and the time it was reached
+        hist = r["history"]
+        k = len(hist)
+        while k > 0 and abs(hist[k - 1][1] - r["energy"]) <= 1e-6:
+            k -= 1
+        k = min(k, len(hist) - 1)
+        out["arms"][label] = {"seconds_to_energy": wall, "iterations": r["iterations"], "converged": r["converged"],
+                              "energy": r["energy"], "dE_vs_fp64_Eh": r["energy"] - ref,
+                              "iterations_to_1e-6": k + 1, "seconds_to_1e-6": t_guess + hist[k][5] * 1e-3,
+                              "full_builds": r["full_builds"], "difference_builds": r["difference_builds"],
+                              "build_seconds": r["build_seconds"], "guess_seconds": t_guess,
+                              "setup_seconds": t_setup}
+        if hook is not None:
+            out["arms"][label]["guess"] = {"accepted": hook["accepted"], "predict_seconds": hook["predict_s"],
+                                           "first_energy_learned": hook["E_first_learned"],
+                                           "first_energy_default": hook["E_first_default"]}
+    model.close()
+    base = out["arms"].get("fp64", {}).get("seconds_to_energy")
+    if base:
+        out["speedup_vs_fp64"] = {k: base / v["seconds_to_energy"] for k, v in out["arms"].items()}
+        b6 = out["arms"]["fp64"]["seconds_to_1e-6"]
+        out["speedup_vs_fp64_to_1e-6"] = {k: b6 / v["seconds_to_1e-6"] for k, v in out["arms"].items()}
+    out["note"] = ("seconds_to_energy: to the reference's convergence tests (|dE| < 1e-10, rms and max dP < 1e-10); "
+                   "below max dP ~1e-8 the loop wanders at the rounding level until one step meets them, so the "
+                   "iteration count of that tail is deterministic for this code but sensitive to any change in "
+                   "rounding; seconds_to_1e-6: until the energy is and stays within 1e-6 Eh of the converged one")
+    return out
+
+
 def ours_arm(args):
     import torch
     import torch.distributed as dist
@@ -324,6 +390,15 @@ def ours_arm(args):
         mixed = {"fp64_gpu_builds_per_s": 1e3 / ms64, "fp64_gpu_ms_per_step": ms64,
                  "speedup_vs_fp64_gpu": ms64 / ms_step, "max_abs_dG_vs_fp64": float(np.abs(dG_).max()),
                  "dE_2e_vs_fp64_Eh": float(0.5 * (Pm * dG_).sum()), "fp32_bound": 1e-8}
+        # how much of the build the FP32 list carries
+        p32 = eng.precision_stats()
+        f32 = sum(P.class_flops(k, v[1]) for k, v in p32.items())
+        mixed["fp32_share_shell_quartets"] = sum(v[0] for v in p32.values()) / max(1, n_shell * world)
+        mixed["fp32_share_flop_alg"] = f32 / max(1.0, flops * world)
+        mixed["fp32_share_per_class"] = {
+            k: {"shell_quartets": round(v[0] / max(1, stats[k][0]), 4),
+                "flop_alg": round(P.class_flops(k, v[1]) / max(1.0, P.class_flops(k, stats[k][1])), 4)}
+            for k, v in sorted(p32.items(), key=lambda kv: -P.class_flops(kv[0], kv[1][1]))[:12]}
 
     # per-class timing pass (events around each class kernel, untimed region)
     dP_host = Pm  # class_stats times a build on the context's current density
@@ -387,6 +462,8 @@ def ours_arm(args):
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = {k: v for k, v in cpu_fock_rate(shells, budget_s=args.cpu_budget).items()
                                     if k != "est_seconds_per_build"}
+        if world == 1 and not args.no_scf:
+            line["time_to_energy"] = time_to_energy(local)
         result = line
         print(json.dumps(line), flush=True)
     eng.close()
@@ -394,6 +471,137 @@ def ours_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0 if result is not None or rank != 0 else 1
+
+
+# ---------------------------------------------------------------------------
+# ERI class microbenchmark: every class (ss|ss)..(ff|ff) on seed-random shell
+# quartets, Obara-Saika and Rys kernels, FP64 and FP32-with-FP64-Boys
+# ---------------------------------------------------------------------------
+CLASS_LS = [(pc_a, pc_b, pk_a, pk_b)
+            for x, (pc_a, pc_b) in enumerate([(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2),
+                                               (3, 3)])
+            for (pk_a, pk_b) in [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3)][:x + 1]]
+
+
+def _oracle_block_check(shells, n_check, blocks, budget_s):
+    """Max |GPU - oracle| over the first quartets of a class (oracle Rys
+    engine, one small oracle basis per group of quartets), within a time
+    budget.  blocks: {variant: (n, ncomp) host array of the same quartets}."""
+    import oracle
+    L = np.asarray(shells["L"])
+    off = np.concatenate([[0], np.cumsum(shells["nprim"])])
+    nbf = int(sum((int(l) + 1) * (int(l) + 2) // 2 for l in L[:4]))
+    group = max(1, min(64, 200 // nbf))
+    t0 = time.perf_counter()
+    worst = {k: 0.0 for k in blocks}
+    within = {k: 0 for k in blocks}
+    ncomp = next(iter(blocks.values())).shape[1]
+    done = 0
+    while done < n_check and time.perf_counter() - t0 < budget_s:
+        g = min(group, n_check - done)
+        s0, s1 = 4 * done, 4 * (done + g)
+        sub = {"L": L[s0:s1], "nprim": shells["nprim"][s0:s1], "center": shells["center"][s0:s1],
+               "expo": shells["expo"][off[s0]:off[s1]], "coef": shells["coef"][off[s0]:off[s1]],
+               "norm": shells["norm"][off[s0]:off[s1]]}
+        ob = oracle.Basis(sub)
+        for k in range(g):
+            ref = ob.shell_block(4 * k, 4 * k + 1, 4 * k + 2, 4 * k + 3, oracle.RYS)
+            for name, blk in blocks.items():
+                d = np.abs(blk[done + k] - ref) / np.maximum(1.0, np.abs(ref))
+                worst[name] = max(worst[name], float(d.max()))
+                within[name] += int((d <= 1e-10).sum())
+        done += g
+    return done, {k: {"max_rel_err": worst[k], "frac_within_1e-10": within[k] / max(1, done * ncomp)}
+                  for k in blocks}
+
+
+def eri_classes(args):
+    """Per-class throughput and accuracy of the integral kernels: 2^20
+    seed-random shell quartets per class (centres in a 10 Angstrom cube,
+    exponents log-uniform in [0.05, 1e4], contraction depth 1..6,
+    coefficients in (0, 1]), through pfk_eri_batch in chunks that fit the
+    device.  Variants: Rys FP64 (the reference for the errors), Rys FP32,
+    and, for L <= 4, Obara-Saika FP64 and FP32.  Times are the kernels' own,
+    from CUDA events on the launching stream."""
+    import torch
+    P = _pfk()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    fp64_peak, fp32_peak = P.measure_fma_peak(0)
+    rows = []
+    classes = CLASS_LS if not args.classes else [CLASS_LS[int(c)] for c in args.classes.split(",")]
+    for (la, lb, lc, ld) in classes:
+        name = "(%s%s|%s%s)" % tuple("spdf"[x] for x in (la, lb, lc, ld))
+        t_gen = time.perf_counter()
+        shells, pairs, quartets = P.workloads.eri_class_quartets(la, lb, lc, ld, args.quartets, seed=SEED)
+        t_gen = time.perf_counter() - t_gen
+        kq = shells["nprim"].reshape(-1, 4).astype(np.int64).prod(axis=1)
+        flops = P.class_flops(name, int(kq.sum()))
+        batch = P.EriBatch(shells, pairs, quartets)
+        nc, n = batch.ncomp, batch.n
+        chunk = int(min(n, max(256, (1 << 30) // (8 * nc))))
+        variants = [("rys", "fp64"), ("rys", "mixed")]
+        if la + lb + lc + ld <= 4:
+            variants += [("os", "fp64"), ("os", "mixed")]
+        bufs = {v: torch.empty(chunk * nc, dtype=torch.float64, device="cuda:0") for v in variants}
+        ms = {v: 0.0 for v in variants}
+        err = {v: 0.0 for v in variants}
+        rel = {v: 0.0 for v in variants}
+        ncheck = min(n, args.oracle_quartets)
+        keep = {v: [] for v in variants if v[1] == "fp64"}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * len(variants))]
+        with torch.cuda.stream(stream):
+            batch.run(0, min(chunk, n), "rys", "fp64", bufs[variants[0]].data_ptr(), stream.cuda_stream)   # warm-up
+            for first in range(0, n, chunk):
+                cnt = min(chunk, n - first)
+                for k, v in enumerate(variants):
+                    ev[2 * k].record(stream)
+                    batch.run(first, cnt, v[0], v[1], bufs[v].data_ptr(), stream.cuda_stream)
+                    ev[2 * k + 1].record(stream)
+                stream.synchronize()
+                for k, v in enumerate(variants):
+                    ms[v] += ev[2 * k].elapsed_time(ev[2 * k + 1])
+                ref = bufs[variants[0]][:cnt * nc]
+                for v in variants[1:]:
+                    d = (bufs[v][:cnt * nc] - ref).abs()
+                    err[v] = max(err[v], float(d.max()))
+                    rel[v] = max(rel[v], float((d / ref.abs().clamp(min=1.0)).max()))
+                if first < ncheck:
+                    for v in keep:
+                        take = min(cnt, ncheck - first)
+                        keep[v].append(bufs[v][:take * nc].view(take, nc).cpu().numpy())
+        batch.close()
+        blocks = {f"{v[0]}_{v[1]}": np.concatenate(keep[v]) for v in keep}
+        n_or, orc = _oracle_block_check(shells, ncheck, blocks, args.oracle_budget)
+        for v in variants:
+            peak = fp64_peak if v[1] == "fp64" else fp32_peak
+            rate = flops / (ms[v] * 1e-3) / 1e12
+            row = {"class": name, "engine": v[0], "arith": "fp64" if v[1] == "fp64" else "fp32+fp64-boys",
+                   "quartets": n, "primitive_quartets": int(kq.sum()), "ms": round(ms[v], 3),
+                   "quartets_per_s": n / (ms[v] * 1e-3), "flop_alg_tflops": rate,
+                   "frac_of_measured_peak": rate / peak,
+                   "peak": "fp64 FMA" if v[1] == "fp64" else "fp32 FMA",
+                   "max_abs_err_vs_rys_fp64": err[v], "max_rel_err_vs_rys_fp64": rel[v]}
+            if v[1] == "fp64":
+                row["oracle"] = dict(orc[f"{v[0]}_{v[1]}"], quartets=n_or)
+            rows.append(row)
+            print(json.dumps(row), flush=True)
+    out = {"what": "ERI class microbenchmark: per-class quartets/s and error, 55 classes x {OS, Rys} x {FP64, "
+                   "FP32 with FP64 Boys/roots}; OS kernels exist for L <= 4",
+           "inputs": f"{args.quartets} seed-random shell quartets per class (seed {SEED}): centres uniform in a "
+                     "10 Angstrom cube, exponents log-uniform in [0.05, 1e4], contraction depth uniform 1..6, "
+                     "coefficients uniform in (0, 1], reference normalisation",
+           "timing": "CUDA events around each kernel launch on its stream, summed over chunks; outputs are the "
+                     "normalised Cartesian blocks written to HBM",
+           "fp64_fma_peak_tflops": fp64_peak, "fp32_fma_peak_tflops": fp32_peak,
+           "oracle": "first quartets of each class against the oracle's per-component Rys integrals "
+                     f"(up to {args.oracle_quartets} quartets or {args.oracle_budget} s per class); "
+                     "relative to max(1, |v|)",
+           "rows": rows}
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(out, f, indent=1)
+    return 0
 
 
 def main():
@@ -410,11 +618,21 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU sampling for cpu_baseline")
     ap.add_argument("--ref-budget", type=float, default=8.0, help="seconds of CPU sampling per reference step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-scf", action="store_true", help="skip the C40H82 time-to-energy leg")
     ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 3, 4],
                     help="streams the class kernels of a build are spread over")
     ap.add_argument("--waters", type=int, default=32,
                     help="cluster size; 32 is the benchmark workload, smaller sizes are for profiling")
+    ap.add_argument("--mode", choices=["fock", "eri-classes"], default="fock",
+                    help="fock: the Fock-build benchmark (default); eri-classes: the ERI class microbenchmark")
+    ap.add_argument("--quartets", type=int, default=1 << 20, help="eri-classes: shell quartets per class")
+    ap.add_argument("--classes", default="", help="eri-classes: comma-separated class indices (default: all 55)")
+    ap.add_argument("--oracle-quartets", type=int, default=4096, help="eri-classes: oracle subset per class")
+    ap.add_argument("--oracle-budget", type=float, default=3.0, help="eri-classes: oracle seconds per class")
+    ap.add_argument("--out", default="", help="eri-classes: JSON file for the table")
     args = ap.parse_args()
+    if args.mode == "eri-classes":
+        return eri_classes(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

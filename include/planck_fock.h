@@ -172,6 +172,11 @@ pfk_status pfk_ump2_energy(pfk_ctx *ctx, const double *Ca, const double *eps_a, 
 pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_quartets55,
                            double *ms55);
 
+/* The FP32 list of the mixed-precision builds per class: its screened shell
+ * quartets and primitive quartets (zero in FP64 mode).  The rest of each
+ * class (pfk_class_stats) runs in FP64.  Any output may be NULL. */
+pfk_status pfk_precision_stats(pfk_ctx *ctx, long long *fp32_quartets55, long long *fp32_prim_quartets55);
+
 /* Restrict every later build of this context to shard `rank` of `nranks`:
  * of each class's screened quartet list (ordered by primitive loop length)
  * only every nranks-th quartet starting at `rank` is evaluated, so the
@@ -196,7 +201,9 @@ pfk_status pfk_set_density_screening(pfk_ctx *ctx, double dtol);
  * tail and the small classes overlap the others.  Classes go, largest
  * (primitive quartets x component quartets) first, to the lane with the
  * least work.  lanes = 1 issues them in class order on the build's stream.
- * The results differ only by the order of the FP64 atomic additions.
+ * The results are bitwise identical for every lane count: the J/K
+ * accumulation is in fixed-point integers, whose sums do not depend on the
+ * order of the additions.
  * Not in the reference (its loop over quartets is one OpenMP region). */
 pfk_status pfk_set_lanes(pfk_ctx *ctx, int lanes);
 
@@ -229,6 +236,84 @@ pfk_status pfk_autotune(pfk_ctx *ctx, int *choice55, double *ms55x3);
  * loop over all SMs, timed with CUDA events.  The FP64 figure is the
  * roofline denominator of the integral kernels. */
 pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
+
+/* ---- ERI batches --------------------------------------------------------
+ * The contracted, normalised Cartesian block of every listed shell quartet,
+ * from the class kernels of the Fock builds, written to device memory
+ * instead of digested: the per-quartet integrals of the reference's
+ * _contracted_eri (os.cpp:994-1010) and _rys_contracted_eri
+ * (rys.cpp:489-505), all components of a shell quartet at once, every
+ * primitive quartet evaluated, no Schwarz screening.  For the per-class
+ * throughput and accuracy measurements of the integral kernels.
+ *
+ * pfk_eri_batch_create: shells as for pfk_create; pair_shells[2p], [2p+1]
+ * are the shells (A, B) of pair p, with L(A) >= L(B).
+ * pfk_eri_batch_set_quartets: host list of (bra pair, ket pair) ids, all of
+ * one class with class(bra) >= class(ket) in the pair-class order ss, ps,
+ * pp, ds, dp, dd, fs, fp, fd, ff; uploads it.  cls (may be NULL) receives
+ * the quartet class (0..54), ncomp the components per quartet.
+ * pfk_eri_batch_run: quartets first .. first+count-1 of the list into d_out
+ * (device, count * ncomp doubles; quartet t's block at t * ncomp, component
+ * ((ia*NB + ib)*NC + ic)*ND + id in the reference's Cartesian order),
+ * asynchronous on `stream` (NULL: the batch's own).  engine: PFK_ENGINE_OS
+ * (classes with LA+LB+LC+LD <= 4; PFK_ERR_UNSUPPORTED above) or
+ * PFK_ENGINE_RYS; precision PFK_PREC_FP64, or PFK_PREC_MIXED for the FP32
+ * variant (recurrences, transfers and contraction in FP32; Boys values, Rys
+ * roots and weights and the per-primitive scalars in FP64). */
+typedef struct pfk_eri_batch pfk_eri_batch;
+pfk_status pfk_eri_batch_create(const pfk_basis_desc *basis, int npairs, const int *pair_shells, int device,
+                                pfk_eri_batch **out);
+pfk_status pfk_eri_batch_destroy(pfk_eri_batch *b);
+const char *pfk_eri_batch_last_error(const pfk_eri_batch *b);
+pfk_status pfk_eri_batch_set_quartets(pfk_eri_batch *b, const int *quartets, long long n, int *cls, int *ncomp);
+pfk_status pfk_eri_batch_run(pfk_eri_batch *b, long long first, long long count, int engine, int precision,
+                             double *d_out, void *stream);
+
+/* ---- RHF on the device -------------------------------------------------
+ * The loop of the reference's run_rhf (src/scf/scf.cpp:175-441) with the
+ * context's Fock builds, all FP64 on the device: symmetric orthogonaliser
+ * X = S^-1/2, the core-Hamiltonian guess (or the caller's P0, taken like the
+ * reference's ReadDensity guess), F = H + G(P), E = 1/2 sum P (H + F) + E_nuc,
+ * Pulay DIIS over the last diis_depth Fock matrices with error
+ * X^T (F P S - S P F) X (types.h:759-837; the small DIIS system solved on
+ * the host by column-pivoted QR), diagonalisation (cuSOLVER Dsyevd),
+ * P = 2 C_occ C_occ^T; converged when |dE| < tol_energy and the rms and max
+ * of the density change are below tol_density, not before iteration 2
+ * (scf.cpp:126-135).  max_iter 0 takes the reference's limit by basis size
+ * (types.h:356-363).  A non-null `incremental` (a second context on the same
+ * basis, normally mixed precision with every quartet on the FP32 list and
+ * density screening) builds G(P) = G(P_built) + G(P - P_built) while
+ * incremental_floor <= max|P - P_built| < incremental_below, with a full
+ * build at least every full_every iterations and one for the final energy;
+ * not in the reference.  G0 (with P0) is the caller's build of the first
+ * iteration (the learned-guess hook makes it).  H, S, P0, G0 and the outputs
+ * P_out, C_out (MO coefficients, column-major), eps_out are host arrays and
+ * may be NULL where optional; the sums are in a fixed order, so a run is
+ * bitwise reproducible. */
+typedef struct {
+    int max_iter;              /* 0: the reference's limit by basis size */
+    double tol_energy;         /* 1e-10 */
+    double tol_density;        /* 1e-10 */
+    int diis_depth;            /* 8 */
+    pfk_ctx *incremental;      /* NULL: full builds only */
+    double incremental_below;  /* 1e-4 */
+    double incremental_floor;  /* 1e-8 */
+    int full_every;            /* 8 */
+    double *history;           /* NULL, or 6 doubles per iteration (host): iteration, E, |dE|, rms dP,
+                                  max dP, milliseconds since the call began */
+} pfk_scf_options;
+
+typedef struct {
+    double energy, first_energy;
+    int iterations, converged;
+    int full_builds, difference_builds;
+    double build_ms;           /* device time of the Fock builds (CUDA events) */
+    double total_ms;           /* wall time of the call */
+} pfk_scf_result;
+
+pfk_status pfk_scf_rhf(pfk_ctx *ctx, const double *H, const double *S, double enuc, int nocc, const double *P0,
+                       const double *G0, const pfk_scf_options *opt, pfk_scf_result *res, double *P_out,
+                       double *C_out, double *eps_out);
 
 /* One-electron integrals of the basis: overlap S, kinetic energy T and
  * nuclear attraction V (nbasis x nbasis, host buffers, symmetric), with
@@ -287,11 +372,14 @@ pfk_status pfk_mlp_train_step(pfk_mlp *m, const float *X, const float *T, int n,
  *   dP, dG  nbasis x nbasis densities / result on the current CUDA device
  *   stream  cudaStream_t for the work (NULL: the default stream); the call
  *           synchronises it and returns with dG written.
- * The first call on a device looks up the scratch array's device address and
- * sets kernel attributes on that device; make that first call before any
- * stream capture.  All calls on a device share the one array: calls that
- * overlap on the GPU (other host threads, other streams) race and must be
- * serialised by the caller.  Each call clears what it needs at zero. */
+ * Every call rebuilds the pair data, the Schwarz table and the screened
+ * quartet list on the host (it copies the Schwarz table back and
+ * synchronises the stream to do so), so it costs host time per call and
+ * must never be called inside a stream capture.  The first call on a device
+ * also looks up the scratch array's device address and sets kernel
+ * attributes on that device.  All calls on a device share the one array:
+ * calls that overlap on the GPU (other host threads, other streams) race and
+ * must be serialised by the caller.  Each call clears what it needs at zero. */
 pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const double *dP, double *dG, double tol_eri,
                                 void *stream);
 

@@ -67,6 +67,10 @@ def lib():
             L.orc_eri_tensor.argtypes = [vp, c_dbl, c_int, vp, vp]
             L.orc_fock_rhf_from_tensor.argtypes = [ctypes.c_size_t, vp, vp, vp]
             L.orc_fock_uhf_from_tensor.argtypes = [ctypes.c_size_t, vp, vp, vp, vp, vp]
+            L.orc_shell_block.restype = None
+            L.orc_shell_block.argtypes = [vp, c_int, c_int, c_int, c_int, c_int, vp]
+            L.orc_fock_elements.restype = None
+            L.orc_fock_elements.argtypes = [vp, c_dbl, c_int, vp, vp, vp, c_int, vp]
             L.orc_jk_direct.restype = ctypes.c_longlong
             L.orc_jk_direct.argtypes = [vp, c_dbl, c_int, vp, c_int, vp, vp, vp, vp, c_int, c_int]
             L.orc_jk_direct_rows.restype = ctypes.c_longlong
@@ -233,6 +237,25 @@ class Basis:
         n = lib().orc_jk_direct_rows(self.h, tol, engine, _p(Q), len(Pk_list), _p(Pj), _p(Pk),
                                      _p(J), _p(K), _p(rows), len(rows))
         return J, K, n
+
+    def shell_block(self, sa, sb, sc, sd, engine=OS):
+        """Cartesian block (sa sb|sc sd), components ((ia*NB+ib)*NC+ic)*ND+id."""
+        L = self.shells["L"]
+        n = [(int(L[x]) + 1) * (int(L[x]) + 2) // 2 for x in (sa, sb, sc, sd)]
+        out = np.zeros(n[0] * n[1] * n[2] * n[3])
+        lib().orc_shell_block(self.h, int(sa), int(sb), int(sc), int(sd), engine, _p(out))
+        return out
+
+    def fock_elements(self, P, elems, tol=1e-10, engine=OS, Q=None):
+        """G(m, n) = J - K/2 of the RHF build for the (m, n) pairs in elems,
+        from the definition (O(nb^2) integrals per element)."""
+        if Q is None:
+            Q = self.schwarz(engine)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        el = np.ascontiguousarray(np.asarray(elems, dtype=np.int32).reshape(-1, 2))
+        out = np.zeros(len(el))
+        lib().orc_fock_elements(self.h, tol, engine, _p(Q), _p(P), _p(el), len(el), _p(out))
+        return out
 
     def row_count(self, p, tol, Q):
         return lib().orc_row_count(self.h, tol, _p(Q), int(p))

@@ -926,6 +926,9 @@ void orc_schwarz(const orc_basis *b, int engine, double *Q)
 {
     const int nb = b->nbasis;
     memset(Q, 0, sizeof(double) * nb * nb);
+    /* The reference runs this loop serially; every element is computed on
+     * its own, so the threads change the time, not the values. */
+#pragma omp parallel for schedule(dynamic, 64)
     for (int p = 0; p < b->npairs; ++p) {
         const orc_pair *sp = &b->pairs[p];
         const double diag = contracted(b, sp, sp, engine == ORC_OS ? ORC_OS : ORC_RYS);
@@ -1094,6 +1097,84 @@ long long orc_jk_direct_rows(const orc_basis *b, double tol, int engine, const d
     return jk_rows(b, tol, engine, Q, nmat, Pj, Pk, J, K, rows, nrows, 0);
 }
 
+/* Index of AO pair (i, j) in the upper-triangle row-major pair order. */
+static inline int pair_index(int nb, int i, int j)
+{
+    if (i > j) {
+        const int t = i;
+        i = j;
+        j = t;
+    }
+    return i * (2 * nb - i + 1) / 2 + (j - i);
+}
+
+/* Selected elements G(m, n) of the RHF two-electron matrix, straight from
+ * its definition over the full index range, G = J - K/2 with
+ * J(m,n) = sum_{r,s} (mn|rs) P(r,s) and K(m,n) = sum_{r,s} (mr|ns) P(r,s)
+ * (the contraction of os.cpp:1512-1520), each integral dropped when its
+ * canonical quartet fails the Schwarz test (os.cpp:1475; the test is
+ * invariant under the 8-fold permutations).  Costs O(nb^2) integrals per
+ * element, so it checks single elements of systems whose full build is far
+ * too slow for the oracle.  elems holds (m, n) pairs. */
+void orc_fock_elements(const orc_basis *b, double tol, int engine, const double *Q, const double *P,
+                       const int *elems, int nelem, double *out)
+{
+    const int nb = b->nbasis;
+    for (int e = 0; e < nelem; ++e) {
+        const int m = elems[2 * e], n = elems[2 * e + 1];
+        const orc_pair *mn = &b->pairs[pair_index(nb, m, n)];
+        const double qmn = Q[m * nb + n];
+        double J = 0.0, K = 0.0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : J, K)
+        for (int r = 0; r < nb; ++r) {
+            /* J: (mn|rs) = (mn|sr) and P is symmetric, so s >= r with weight 2 off the diagonal */
+            for (int s = r; s < nb; ++s) {
+                if (qmn * Q[r * nb + s] < tol)
+                    continue;
+                const double v = contracted(b, mn, &b->pairs[pair_index(nb, r, s)], engine);
+                J += (s == r ? 1.0 : 2.0) * v * P[r * nb + s];
+            }
+            /* K: (mr|ns) for every s */
+            const double qmr = Q[m * nb + r];
+            const orc_pair *mr = &b->pairs[pair_index(nb, m, r)];
+            for (int s = 0; s < nb; ++s) {
+                if (qmr * Q[n * nb + s] < tol)
+                    continue;
+                K += contracted(b, mr, &b->pairs[pair_index(nb, n, s)], engine) * P[r * nb + s];
+            }
+        }
+        out[e] = J - 0.5 * K;
+    }
+}
+
+/* The contracted Cartesian block of one shell quartet (sa sb|sc sd) without
+ * screening: out[((ia*NB + ib)*NC + ic)*ND + id] = (i j|k l) for the AOs of the
+ * four shells in the reference's component order, each from the per-component
+ * contraction of os.cpp:994-1010 / rys.cpp:489-505. */
+void orc_shell_block(const orc_basis *b, int sa, int sb, int sc, int sd, int engine, double *out)
+{
+    const int nb = b->nbasis;
+    const int sh[4] = {sa, sb, sc, sd};
+    int first[4], n[4];
+    for (int q = 0; q < 4; ++q) {
+        first[q] = -1;
+        for (int k = 0; k < nb && first[q] < 0; ++k)
+            if (b->ao[k].shell == sh[q])
+                first[q] = k;
+        n[q] = (b->L[sh[q]] + 1) * (b->L[sh[q]] + 2) / 2;
+    }
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int ia = 0; ia < n[0]; ++ia)
+        for (int ib = 0; ib < n[1]; ++ib) {
+            const orc_pair *ab = &b->pairs[pair_index(nb, first[0] + ia, first[1] + ib)];
+            for (int ic = 0; ic < n[2]; ++ic)
+                for (int id = 0; id < n[3]; ++id) {
+                    const orc_pair *cd = &b->pairs[pair_index(nb, first[2] + ic, first[3] + id)];
+                    out[((ia * n[1] + ib) * n[2] + ic) * n[3] + id] = contracted(b, ab, cd, engine);
+                }
+        }
+}
+
 /* Number of screened canonical AO quartets in bra row p (q >= p). */
 long long orc_row_count(const orc_basis *b, double tol, const double *Q, int p)
 {
@@ -1133,6 +1214,33 @@ long long orc_quartet_list(const orc_basis *b, double tol, const double *Q, uint
     const int nb = b->nbasis;
     long long count = 0;
     uint64_t h = 0;
+    if (!out) {
+        /* count and digest only: the digest is a sum of per-quartet hashes,
+         * so threads over the bra pairs give the serial loop's exact result;
+         * the pairs' Q values and codes are gathered into arrays first */
+        const int np = b->npairs;
+        double *qv = (double *)malloc(sizeof(double) * (size_t)(np > 0 ? np : 1));
+        uint64_t *code = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(np > 0 ? np : 1));
+        for (int p = 0; p < np; ++p) {
+            qv[p] = Q[b->pairs[p].i * nb + b->pairs[p].j];
+            code[p] = orc_quartet_code(b->pairs[p].i, b->pairs[p].j, 0, 0);
+        }
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : count, h)
+        for (int p = 0; p < np; ++p) {
+            const double qab = qv[p];
+            const uint64_t cab = code[p];
+            for (int q = p; q < np; ++q) {
+                if (qab * qv[q] < tol)
+                    continue;
+                h += mix64(cab | (code[q] >> 32));
+                ++count;
+            }
+        }
+        free(qv);
+        free(code);
+        *digest = h;
+        return count;
+    }
     for (int p = 0; p < b->npairs; ++p) {
         const orc_pair *ab = &b->pairs[p];
         for (int q = p; q < b->npairs; ++q) {

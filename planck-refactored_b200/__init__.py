@@ -35,7 +35,8 @@ EXPORTS = ["pfk_create", "pfk_destroy", "pfk_set_options", "pfk_nbasis", "pfk_la
            "pfk_mlp_train_step", "pfk_checkpoint_write", "pfk_checkpoint_read_density",
            "pfk_checkpoint_last_error", "pfk_mo_transform",
            "pfk_mo_transform_times", "pfk_rmp2_energy",
-           "pfk_ump2_energy"]
+           "pfk_ump2_energy", "pfk_eri_batch_create", "pfk_eri_batch_destroy", "pfk_eri_batch_last_error",
+           "pfk_eri_batch_set_quartets", "pfk_eri_batch_run", "pfk_precision_stats", "pfk_scf_rhf"]
 
 _lib = None
 
@@ -44,6 +45,19 @@ class PfkError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"pfk status {status}: {msg}")
         self.status = status
+
+
+class ScfOptions(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("tol_energy", ctypes.c_double), ("tol_density", ctypes.c_double),
+                ("diis_depth", ctypes.c_int), ("incremental", ctypes.c_void_p),
+                ("incremental_below", ctypes.c_double), ("incremental_floor", ctypes.c_double),
+                ("full_every", ctypes.c_int), ("history", ctypes.c_void_p)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("first_energy", ctypes.c_double), ("iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("full_builds", ctypes.c_int), ("difference_builds", ctypes.c_int),
+                ("build_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
 
 
 class BasisDesc(ctypes.Structure):
@@ -92,6 +106,15 @@ def load_library(path=LIB_PATH):
     L.pfk_ump2_energy.argtypes = [vp, vp, vp, vp, vp, c_int, c_int, ctypes.POINTER(c_dbl)]
     L.pfk_set_primitive_tol.argtypes = [vp, c_dbl]
     L.pfk_autotune.argtypes = [vp, vp, vp]
+    L.pfk_precision_stats.argtypes = [vp, vp, vp]
+    L.pfk_scf_rhf.argtypes = [vp, vp, vp, c_dbl, c_int, vp, vp, ctypes.POINTER(ScfOptions),
+                              ctypes.POINTER(ScfResult), vp, vp, vp]
+    L.pfk_eri_batch_create.argtypes = [ctypes.POINTER(BasisDesc), c_int, vp, c_int, ctypes.POINTER(vp)]
+    L.pfk_eri_batch_destroy.argtypes = [vp]
+    L.pfk_eri_batch_last_error.restype = ctypes.c_char_p
+    L.pfk_eri_batch_last_error.argtypes = [vp]
+    L.pfk_eri_batch_set_quartets.argtypes = [vp, vp, c_ll, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
+    L.pfk_eri_batch_run.argtypes = [vp, c_ll, c_ll, c_int, c_int, vp, vp]
     _lib = L
     return L
 
@@ -252,8 +275,42 @@ class FockEngine:
         self._check(self.lib.pfk_class_stats(self.h, _p(q), _p(k), _p(ms) if timed else None))
         return {CLASS_NAMES[c]: (int(q[c]), int(k[c]), float(ms[c])) for c in range(55) if q[c]}
 
+    def precision_stats(self):
+        """{class name: (FP32 shell quartets, FP32 primitive quartets)} for the
+        classes with a non-empty FP32 list (mixed precision)."""
+        q = np.zeros(55, dtype=np.int64)
+        k = np.zeros(55, dtype=np.int64)
+        self._check(self.lib.pfk_precision_stats(self.h, _p(q), _p(k)))
+        return {CLASS_NAMES[c]: (int(q[c]), int(k[c])) for c in range(55) if q[c]}
+
     def set_shard(self, rank, nranks):
         self._check(self.lib.pfk_set_shard(self.h, int(rank), int(nranks)))
+
+    def scf_rhf(self, H, S, enuc, nocc, P0=None, G0=None, max_iter=0, tol_energy=1e-10, tol_density=1e-10,
+                diis_depth=8, incremental=None, incremental_below=1e-4, incremental_floor=1e-8, full_every=8):
+        """RHF to convergence on the device (pfk_scf_rhf).  incremental: an
+        optional second FockEngine for the difference-density builds.
+        Returns scf.rhf()'s dict keys (energy, iterations, converged, P, C,
+        eps, first_energy) plus the build counts and times."""
+        nb = self.nbasis
+        H, S = _f64(H), _f64(S)
+        P0 = None if P0 is None else _f64(P0)
+        G0 = None if G0 is None else _f64(G0)
+        mi = int(max_iter or 0) or (300 if nb > 1000 else 200 if nb > 500 else 100 if nb > 250 else 50)
+        hist = np.zeros((mi, 6))
+        opt = ScfOptions(mi, tol_energy, tol_density, int(diis_depth),
+                         incremental.h if incremental is not None else None, incremental_below, incremental_floor,
+                         int(full_every), _p(hist))
+        res = ScfResult()
+        Pout, Cout, eps = np.zeros((nb, nb)), np.zeros((nb, nb)), np.zeros(nb)
+        self._check(self.lib.pfk_scf_rhf(self.h, _p(H), _p(S), float(enuc), int(nocc),
+                                         None if P0 is None else _p(P0), None if G0 is None else _p(G0),
+                                         ctypes.byref(opt), ctypes.byref(res), _p(Pout), _p(Cout), _p(eps)))
+        return {"energy": res.energy, "first_energy": res.first_energy, "iterations": res.iterations,
+                "converged": bool(res.converged), "P": Pout, "C": Cout.T.copy(), "eps": eps,
+                "full_builds": res.full_builds, "difference_builds": res.difference_builds,
+                "build_seconds": res.build_ms * 1e-3, "seconds": res.total_ms * 1e-3,
+                "history": [tuple(h) for h in hist[:res.iterations]]}
 
     def autotune(self):
         """Measure the candidate kernels per class (pfk_autotune) and keep the
@@ -295,6 +352,50 @@ def _basis_desc(shells):
     desc = BasisDesc(len(keep["L"]), _p(keep["L"]), _p(keep["nprim"]), _p(keep["center"]), _p(keep["expo"]),
                      _p(keep["coef"]), _p(keep["norm"]))
     return desc, keep
+
+
+class EriBatch:
+    """Cartesian blocks of listed shell quartets (pfk_eri_batch_*).
+
+    shells: a shells dict; pairs: (npairs, 2) shell indices with L(first) >=
+    L(second); quartets: (n, 2) pair ids, all of one class (bra class >= ket
+    class).  run() writes blocks into a device buffer given by pointer."""
+
+    def __init__(self, shells, pairs, quartets, device=0):
+        self.lib = load_library()
+        desc, keep = _basis_desc(shells)
+        pr = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        self.h = ctypes.c_void_p()
+        st = self.lib.pfk_eri_batch_create(ctypes.byref(desc), len(pr), _p(pr), int(device), ctypes.byref(self.h))
+        if st != PFK_OK:
+            raise PfkError(st, self.lib.pfk_eri_batch_last_error(None).decode())
+        q = np.ascontiguousarray(quartets, dtype=np.int32).reshape(-1, 2)
+        cls, nc = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.pfk_eri_batch_set_quartets(self.h, _p(q), len(q), ctypes.byref(cls), ctypes.byref(nc)))
+        self.n, self.cls, self.ncomp = len(q), cls.value, nc.value
+        self.name = CLASS_NAMES[self.cls]
+
+    def _check(self, st):
+        if st != PFK_OK:
+            raise PfkError(st, self.lib.pfk_eri_batch_last_error(self.h).decode())
+
+    def run(self, first, count, engine, precision, out_ptr, stream_ptr=0):
+        """Blocks of quartets first..first+count-1 into the device buffer at
+        out_ptr (count * ncomp doubles); asynchronous on the stream."""
+        self._check(self.lib.pfk_eri_batch_run(self.h, int(first), int(count), ENGINES[engine],
+                                               PRECISIONS[precision], ctypes.c_void_p(out_ptr),
+                                               ctypes.c_void_p(stream_ptr)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pfk_eri_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def one_electron(shells, coords, charges, device=0):

@@ -32,6 +32,7 @@ DEPS = {
     "pfk_onee.cu": DEVICE_DEPS + ["pfk_kernels.cuh", "pfk_os.cuh"],
     "pfk_mlp.cu": ["../../include/planck_fock.h"],
     "pfk_checkpoint.cu": ["../../include/planck_fock.h"],
+    "pfk_scf.cu": ["../../include/planck_fock.h", "pfk_internal.h", "pfk_device.cuh"],
 }
 
 
@@ -45,7 +46,7 @@ def _units():
     units = [("pfk_classes.cu", f"classes_{b}_{e}.o", [f"-DPFK_CLASS_BEGIN={b}", f"-DPFK_CLASS_END={e}"])
              for b, e in reversed(CLASS_UNITS)]
     units += [("pfk_setup.cu", "setup.o", []), ("pfk_api.cu", "api.o", []), ("pfk_onee.cu", "onee.o", []),
-              ("pfk_mlp.cu", "mlp.o", []), ("pfk_checkpoint.cu", "checkpoint.o", [])]
+              ("pfk_mlp.cu", "mlp.o", []), ("pfk_checkpoint.cu", "checkpoint.o", []), ("pfk_scf.cu", "scf.o", [])]
     return units
 
 
@@ -79,7 +80,7 @@ def build(jobs=None, force=False, verbose=False):
                 logs[futs[f][1]] = f.result()
     objs = [os.path.join(BUILD, o) for _, o, _ in _units()]
     if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcublas"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcublas", "-lcusolver"]
         subprocess.check_call(cmd)
     return LIB, logs
 

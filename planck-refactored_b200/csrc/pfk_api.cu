@@ -98,6 +98,7 @@ struct pfk_ctx {
     DevBuf<long long> d_cls_kpref[kPairClasses];   // prefix of nprim over the sorted class list
 
     long long prim_cnt[kQuartetClasses] = {};   // primitive quartets (all primitives), per class
+    long long prim32_cnt[kQuartetClasses] = {}; // the part of prim_cnt on the FP32 list
     int shard_rank = 0, shard_n = 1;             // builds evaluate every shard_n-th quartet
 
     double tol = 1e-10, fp32_bound = 1e-8;
@@ -113,7 +114,8 @@ struct pfk_ctx {
     // Rys); the static rule until pfk_autotune measures the candidates
     int auto_flags[kQuartetClasses] = {};
 
-    DevBuf<double> d_P, d_Pb, d_Pt, d_J, d_K0, d_K1, d_G, d_Gb;
+    DevBuf<double> d_P, d_Pb, d_Pt, d_G, d_Gb;
+    DevBuf<FxWord> d_J, d_K0, d_K1;   // fixed-point accumulators, 2 nb^2 words each
     std::vector<GraphEntry> graphs;
 
     pfk_status fail(pfk_status s, const std::string &msg)
@@ -180,6 +182,45 @@ pfk_status validate(const pfk_basis_desc *b, std::string &why)
 
 // Shell pairs a <= b with primitive-pair data (src/base/types.h:631-674),
 // oriented so that L(A) >= L(B).
+//
+// One oriented pair (A, B), L(A) >= L(B): appends its PairInfo and its
+// primitive pairs (qp left at `qp`) to the vectors.  poff: first primitive
+// of each shell.
+void append_pair(const pfk_basis_desc *b, const std::vector<int> &poff, int A, int B, int bf_a, int bf_b, double qp,
+                 std::vector<PairInfo> &pairs, std::vector<PrimPair> &prims)
+{
+    const double *ca = b->center + 3 * A, *cb = b->center + 3 * B;
+    PairInfo pi{};
+    pi.prim_off = (int)prims.size();
+    pi.bf_a = bf_a;
+    pi.bf_b = bf_b;
+    pi.ABx = ca[0] - cb[0];
+    pi.ABy = ca[1] - cb[1];
+    pi.ABz = ca[2] - cb[2];
+    const double R2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+    for (int ia = 0; ia < b->nprim[A]; ++ia)
+        for (int ib = 0; ib < b->nprim[B]; ++ib) {
+            const double alpha = b->expo[poff[A] + ia], beta = b->expo[poff[B] + ib];
+            const double zeta = alpha + beta, iz = 1.0 / zeta;
+            PrimPair p{};
+            p.zeta = zeta;
+            p.inv_zeta = iz;
+            p.Px = (alpha * ca[0] + beta * cb[0]) * iz;
+            p.Py = (alpha * ca[1] + beta * cb[1]) * iz;
+            p.Pz = (alpha * ca[2] + beta * cb[2]) * iz;
+            p.PAx = p.Px - ca[0];
+            p.PAy = p.Py - ca[1];
+            p.PAz = p.Pz - ca[2];
+            const double K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) * b->coef[poff[A] + ia] *
+                             b->coef[poff[B] + ib] * b->norm[poff[A] + ia] * b->norm[poff[B] + ib];
+            p.Kz = K * std::sqrt(zeta);
+            p.qp = qp;
+            prims.push_back(p);
+        }
+    pi.nprim_full = pi.nprim = (int)prims.size() - pi.prim_off;
+    pairs.push_back(pi);
+}
+
 void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
 {
     std::vector<int> poff(b->nshell + 1, 0);
@@ -190,41 +231,8 @@ void build_pairs(pfk_ctx *ctx, const pfk_basis_desc *b)
         for (int sb = sa; sb < b->nshell; ++sb) {
             const int A = b->L[sa] >= b->L[sb] ? sa : sb;
             const int B = A == sa ? sb : sa;
-            const double *ca = b->center + 3 * A, *cb = b->center + 3 * B;
-            PairInfo pi{};
-            pi.prim_off = (int)ctx->prims.size();
-            pi.nprim = b->nprim[A] * b->nprim[B];
-            pi.bf_a = ctx->bf_off[A];
-            pi.bf_b = ctx->bf_off[B];
-            pi.ABx = ca[0] - cb[0];
-            pi.ABy = ca[1] - cb[1];
-            pi.ABz = ca[2] - cb[2];
-            const double R2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
-            std::vector<PrimPair> pp;
-            pp.reserve(pi.nprim);
-            for (int ia = 0; ia < b->nprim[A]; ++ia)
-                for (int ib = 0; ib < b->nprim[B]; ++ib) {
-                    const double alpha = b->expo[poff[A] + ia], beta = b->expo[poff[B] + ib];
-                    const double zeta = alpha + beta, iz = 1.0 / zeta;
-                    PrimPair p{};
-                    p.zeta = zeta;
-                    p.inv_zeta = iz;
-                    p.Px = (alpha * ca[0] + beta * cb[0]) * iz;
-                    p.Py = (alpha * ca[1] + beta * cb[1]) * iz;
-                    p.Pz = (alpha * ca[2] + beta * cb[2]) * iz;
-                    p.PAx = p.Px - ca[0];
-                    p.PAy = p.Py - ca[1];
-                    p.PAz = p.Pz - ca[2];
-                    const double K = std::pow(kPi * iz, 1.5) * std::exp(-alpha * beta * iz * R2) *
-                                     b->coef[poff[A] + ia] * b->coef[poff[B] + ib] * b->norm[poff[A] + ia] *
-                                     b->norm[poff[B] + ib];
-                    p.Kz = K * std::sqrt(zeta);
-                    p.qp = 0.0;   // prim_bounds sets it and orders the pair's primitives
-                    pp.push_back(p);
-                }
-            pi.nprim_full = pi.nprim = (int)pp.size();
-            ctx->prims.insert(ctx->prims.end(), pp.begin(), pp.end());
-            ctx->pairs.push_back(pi);
+            // qp: prim_bounds sets it and orders the pair's primitives
+            append_pair(b, poff, A, B, ctx->bf_off[A], ctx->bf_off[B], 0.0, ctx->pairs, ctx->prims);
             ctx->pair_pc.push_back(pair_class(b->L[A], b->L[B]));
             ctx->pair_la.push_back(b->L[A]);
             ctx->pair_lb.push_back(b->L[B]);
@@ -317,7 +325,7 @@ pfk_status build_lists(pfk_ctx *ctx)
             const int cls = quartet_class(x, y);
             const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
             ctx->q_cnt[cls] = ctx->q32_cnt[cls] = 0;
-            ctx->prim_cnt[cls] = 0;
+            ctx->prim_cnt[cls] = ctx->prim32_cnt[cls] = 0;
             if (nX == 0 || nY == 0) continue;
             PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
                                   cnt_lo.p, ctx->stream));
@@ -364,9 +372,11 @@ pfk_status build_lists(pfk_ctx *ctx)
             PFK_CK(cudaMemcpyAsync(h.data(), work_hi.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
             PFK_CK(cudaMemcpyAsync(h.data() + nX, work_lo.p, sizeof(long long) * nX, cudaMemcpyDeviceToHost, ctx->stream));
             PFK_CK(cudaStreamSynchronize(ctx->stream));
-            long long w = 0;
+            long long w = 0, w32 = 0;
             for (size_t a = 0; a < h.size(); ++a) w += h[a];
+            for (int a = 0; a < nX; ++a) w32 += h[(size_t)nX + a];
             ctx->prim_cnt[cls] = w;
+            ctx->prim32_cnt[cls] = w32;
         }
     // order each list by its primitive loop lengths (stable: bra-major within a key)
     long long maxseg = 1;
@@ -477,14 +487,14 @@ static int class_components(int c)
 
 // Launch every class kernel over the screened lists.  Jacc/K accumulators are
 // zeroed first.  eri_out selects the dense-tensor mode.
-pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const double *Pk1, int nk, double *Jacc,
-                       double *K0, double *K1, double *eri_out, cudaStream_t st, bool timed)
+pfk_status run_classes(pfk_ctx *ctx, const double *Pj, const double *Pk0, const double *Pk1, int nk, FxWord *Jacc,
+                       FxWord *K0, FxWord *K1, double *eri_out, cudaStream_t st, bool timed)
 {
     const size_t nb2 = (size_t)ctx->nb * ctx->nb;
     if (!eri_out) {
-        PFK_CK(cudaMemsetAsync(Jacc, 0, sizeof(double) * nb2, st));
-        if (K0) PFK_CK(cudaMemsetAsync(K0, 0, sizeof(double) * nb2, st));
-        if (K1) PFK_CK(cudaMemsetAsync(K1, 0, sizeof(double) * nb2, st));
+        PFK_CK(cudaMemsetAsync(Jacc, 0, sizeof(FxWord) * 2 * nb2, st));
+        if (K0) PFK_CK(cudaMemsetAsync(K0, 0, sizeof(FxWord) * 2 * nb2, st));
+        if (K1) PFK_CK(cudaMemsetAsync(K1, 0, sizeof(FxWord) * 2 * nb2, st));
     }
     JKArgs a{};
     if (ctx->dscreen_tol > 0.0 && !eri_out) {
@@ -581,8 +591,10 @@ pfk_status ensure_work(pfk_ctx *ctx)
 {
     const size_t nb2 = (size_t)ctx->nb * ctx->nb;
     if (ctx->d_J.p) return PFK_OK;
-    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
+    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_G, &ctx->d_Gb})
         PFK_CK(b->alloc(nb2));
+    for (DevBuf<FxWord> *b : {&ctx->d_J, &ctx->d_K0, &ctx->d_K1})
+        PFK_CK(b->alloc(2 * nb2));
     return PFK_OK;
 }
 
@@ -726,8 +738,8 @@ pfk_status pfk_destroy(pfk_ctx *ctx)
     ctx->d_shell_bf.release();
     ctx->d_shell_nbf.release();
     ctx->d_Dsh.release();
-    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_J, &ctx->d_K0, &ctx->d_K1, &ctx->d_G, &ctx->d_Gb})
-        b->release();
+    for (DevBuf<double> *b : {&ctx->d_P, &ctx->d_Pb, &ctx->d_Pt, &ctx->d_G, &ctx->d_Gb}) b->release();
+    for (DevBuf<FxWord> *b : {&ctx->d_J, &ctx->d_K0, &ctx->d_K1}) b->release();
     for (int i = 0; i < kMaxLanes - 1; ++i) {
         if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
         if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
@@ -956,8 +968,9 @@ pfk_status pfk_eri_tensor(pfk_ctx *ctx, double *eri)
 //   kMp2Same (O - O_ibja)^2 / (4 D)     UMP2 same spin (mp2.cpp:93-124)
 //   kMp2Opp  O^2 / D                    UMP2 opposite spin (mp2.cpp:126-139)
 // O_ibja needs n1 = n3 and n2 = n4.  Grid-stride over the block, a
-// warp-shuffle and shared-memory reduction per block, one FP64 atomic per
-// block into *out (zeroed by the caller).
+// warp-shuffle and shared-memory reduction per block into out[blockIdx.x];
+// the host adds the per-block sums in block order, so the result does not
+// depend on the order in which blocks finish.
 constexpr int kMp2R = 0, kMp2Same = 1, kMp2Opp = 2;
 __global__ void __launch_bounds__(256) mp2_sum_kernel(const double *__restrict__ O, const double *__restrict__ e1,
                                                       const double *__restrict__ e2, int n1, int n2, int n3, int n4,
@@ -987,7 +1000,7 @@ __global__ void __launch_bounds__(256) mp2_sum_kernel(const double *__restrict__
     if (threadIdx.x == 0) {
         double tot = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += part[w];
-        atomicAdd(out, tot);
+        out[blockIdx.x] = tot;
     }
 }
 
@@ -1058,17 +1071,23 @@ static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C
     if (s != PFK_OK) return s;
     PFK_CK(cudaEventRecord(ev[2], st));
     if (eps1) {
+        int nsm = 0;
+        PFK_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+        const int grid = 8 * std::max(nsm, 1);   // 8 blocks of 256 per SM
         DevBuf<double> d_eps, d_sum;
         PFK_CK(d_eps.alloc(2 * b));
-        PFK_CK(d_sum.alloc(1));
+        PFK_CK(d_sum.alloc(grid));
         PFK_CK(cudaMemcpyAsync(d_eps.p, eps1, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
         PFK_CK(cudaMemcpyAsync(d_eps.p + nb, eps2, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
-        PFK_CK(cudaMemsetAsync(d_sum.p, 0, sizeof(double), st));
-        mp2_sum_kernel<<<148 * 8, 256, 0, st>>>(O, d_eps.p, d_eps.p + nb, n1, n2, n3, n4, mode, d_sum.p);
+        mp2_sum_kernel<<<grid, 256, 0, st>>>(O, d_eps.p, d_eps.p + nb, n1, n2, n3, n4, mode, d_sum.p);
         PFK_CK(cudaGetLastError());
-        PFK_CK(cudaMemcpyAsync(e_corr, d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        std::vector<double> part(grid);
+        PFK_CK(cudaMemcpyAsync(part.data(), d_sum.p, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
         PFK_CK(cudaEventRecord(ev[3], st));
         PFK_CK(cudaStreamSynchronize(st));
+        double tot = 0.0;
+        for (int k = 0; k < grid; ++k) tot += part[k];
+        *e_corr = tot;
     } else {
         // the caller's buffer is pageable: stage it through two pinned chunks,
         // so the device copy runs at pinned speed and the host copy of one
@@ -1168,6 +1187,17 @@ pfk_status pfk_class_stats(pfk_ctx *ctx, long long *quartets55, long long *prim_
     for (int c = 0; c < kQuartetClasses; ++c) {
         if (quartets55) quartets55[c] = ctx->q_cnt[c] + ctx->q32_cnt[c];
         if (prim_quartets55) prim_quartets55[c] = ctx->prim_cnt[c];
+    }
+    return PFK_OK;
+}
+
+pfk_status pfk_precision_stats(pfk_ctx *ctx, long long *fp32_quartets55, long long *fp32_prim_quartets55)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        const bool mixed = ctx->precision == PFK_PREC_MIXED;
+        if (fp32_quartets55) fp32_quartets55[c] = mixed ? ctx->q32_cnt[c] : 0;
+        if (fp32_prim_quartets55) fp32_prim_quartets55[c] = mixed ? ctx->prim32_cnt[c] : 0;
     }
     return PFK_OK;
 }
@@ -1429,8 +1459,8 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
     need = carve_size<PrimPair>(need, h.prims.size());
     need = carve_size<int>(need, h.npairs);
     need = carve_size<double>(need, nb2);
-    need = carve_size<double>(need, nb2);
-    need = carve_size<double>(need, nb2);
+    need = carve_size<FxWord>(need, 2 * nb2);
+    need = carve_size<FxWord>(need, 2 * nb2);
     if (need > PFK_NOALLOC_SCRATCH_BYTES) {
         g_last_error = "pfk_fock_rhf_noalloc: basis needs " + std::to_string(need) +
                        " bytes of scratch before the quartet list; the limit is " +
@@ -1442,8 +1472,8 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
     PrimPair *d_prims = cv.take<PrimPair>(h.prims.size());
     int *d_ids = cv.take<int>(h.npairs);
     double *d_Q = cv.take<double>(nb2);
-    double *d_J = cv.take<double>(nb2);
-    double *d_K = cv.take<double>(nb2);
+    FxWord *d_J = cv.take<FxWord>(2 * nb2);
+    FxWord *d_K = cv.take<FxWord>(2 * nb2);
 
 #define PFK_NA_CK(call)                                                                           \
     do {                                                                                         \
@@ -1520,8 +1550,8 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
         PFK_NA_CK(cudaMemcpyAsync(d_q, quart.data(), sizeof(uint2) * quart.size(), cudaMemcpyHostToDevice, st));
 
     // the build: accumulators start at zero on every call
-    PFK_NA_CK(cudaMemsetAsync(d_J, 0, sizeof(double) * nb2, st));
-    PFK_NA_CK(cudaMemsetAsync(d_K, 0, sizeof(double) * nb2, st));
+    PFK_NA_CK(cudaMemsetAsync(d_J, 0, sizeof(FxWord) * 2 * nb2, st));
+    PFK_NA_CK(cudaMemsetAsync(d_K, 0, sizeof(FxWord) * 2 * nb2, st));
     JKArgs a{};
     a.pairs = d_pairs;
     a.prims = d_prims;
@@ -1545,3 +1575,213 @@ extern "C" pfk_status pfk_fock_rhf_noalloc(const pfk_basis_desc *basis, const do
 #undef PFK_NA_CK
     return PFK_OK;
 }
+
+// ===========================================================================
+// ERI batches (pfk_eri_batch_*): the contracted, normalised Cartesian block
+// of every listed shell quartet, from the same class kernels the Fock builds
+// use, written out instead of digested.  For the per-class measurements and
+// accuracy tables of the integral kernels (the reference's per-quartet
+// contracted integrals, os.cpp:994-1010 and rys.cpp:489-505).
+// ===========================================================================
+struct pfk_eri_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<int> L;        // per shell
+    std::vector<int> pair_pc;  // per pair
+    DevBuf<PairInfo> d_pairs;
+    DevBuf<PrimPair> d_prims;
+    DevBuf<uint2> d_quart;
+    long long nq = 0;
+    int cls = -1;              // class of the listed quartets
+
+    pfk_status fail(pfk_status s, const std::string &msg)
+    {
+        err = msg;
+        return s;
+    }
+    pfk_status cuda_fail(const char *what, cudaError_t e)
+    {
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return PFK_ERR_CUDA;
+    }
+};
+
+extern "C" {
+
+pfk_status pfk_eri_batch_create(const pfk_basis_desc *basis, int npairs, const int *pair_shells, int device,
+                                pfk_eri_batch **out)
+{
+    if (!out) {
+        g_last_error = "pfk_eri_batch_create: out is null";
+        return PFK_ERR_INVALID;
+    }
+    *out = nullptr;
+    std::string why;
+    pfk_status vs = validate(basis, why);
+    if (vs != PFK_OK) {
+        g_last_error = "pfk_eri_batch_create: " + why;
+        return vs;
+    }
+    if (npairs <= 0 || !pair_shells) {
+        g_last_error = "pfk_eri_batch_create: no shell pairs";
+        return PFK_ERR_INVALID;
+    }
+    std::vector<int> poff(basis->nshell + 1, 0);
+    for (int s = 0; s < basis->nshell; ++s) poff[s + 1] = poff[s] + basis->nprim[s];
+    std::vector<PairInfo> pairs;
+    std::vector<PrimPair> prims;
+    std::vector<int> pc;
+    try {
+        pairs.reserve(npairs);
+        pc.reserve(npairs);
+        for (int p = 0; p < npairs; ++p) {
+            const int A = pair_shells[2 * p], B = pair_shells[2 * p + 1];
+            if (A < 0 || B < 0 || A >= basis->nshell || B >= basis->nshell) {
+                g_last_error = "pfk_eri_batch_create: pair " + std::to_string(p) + " names a shell out of range";
+                return PFK_ERR_INVALID;
+            }
+            if (basis->L[A] < basis->L[B]) {
+                g_last_error = "pfk_eri_batch_create: pair " + std::to_string(p) +
+                               " must list the shell of higher angular momentum first";
+                return PFK_ERR_INVALID;
+            }
+            if ((long long)prims.size() + (long long)basis->nprim[A] * basis->nprim[B] > INT32_MAX) {
+                g_last_error = "pfk_eri_batch_create: more than 2^31 primitive pairs";
+                return PFK_ERR_UNSUPPORTED;
+            }
+            // qp = 1 and no primitive floor: every primitive quartet is evaluated
+            append_pair(basis, poff, A, B, 0, 0, 1.0, pairs, prims);
+            pairs.back().qmax = pairs.back().qmin = 1.0;
+            pc.push_back(pair_class(basis->L[A], basis->L[B]));
+        }
+    } catch (const std::bad_alloc &) {
+        g_last_error = "pfk_eri_batch_create: host allocation failed";
+        return PFK_ERR_NOMEM;
+    }
+    pfk_eri_batch *ctx = new (std::nothrow) pfk_eri_batch();
+    if (!ctx) {
+        g_last_error = "pfk_eri_batch_create: host allocation failed";
+        return PFK_ERR_NOMEM;
+    }
+    auto bail = [&](pfk_status s) {
+        g_last_error = "pfk_eri_batch_create: " + ctx->err;
+        pfk_eri_batch_destroy(ctx);
+        return s;
+    };
+    ctx->device = device;
+    ctx->L.assign(basis->L, basis->L + basis->nshell);
+    ctx->pair_pc = std::move(pc);
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaSetDevice", e));
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(ctx->cuda_fail("cudaStreamCreate", e));
+    // the split and team kernels' shared-memory limits on this device
+    JKArgs none{};
+    for (int c = 0; c < kQuartetClasses; ++c) {
+        if (!g_class_launchers[c]) return bail(ctx->fail(PFK_ERR_STATE, "class kernel table incomplete"));
+        g_class_launchers[c](nullptr, -1, none, 1, 0, nullptr);
+    }
+    if ((e = ctx->d_pairs.alloc(pairs.size())) != cudaSuccess) return bail(ctx->cuda_fail("cudaMalloc(pairs)", e));
+    if ((e = ctx->d_prims.alloc(prims.size())) != cudaSuccess) return bail(ctx->cuda_fail("cudaMalloc(prims)", e));
+    e = cudaMemcpyAsync(ctx->d_pairs.p, pairs.data(), sizeof(PairInfo) * pairs.size(), cudaMemcpyHostToDevice,
+                        ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->d_prims.p, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return bail(ctx->cuda_fail("upload of pair data", e));
+    *out = ctx;
+    return PFK_OK;
+}
+
+pfk_status pfk_eri_batch_destroy(pfk_eri_batch *b)
+{
+    if (!b) return PFK_OK;
+    cudaSetDevice(b->device);
+    b->d_pairs.release();
+    b->d_prims.release();
+    b->d_quart.release();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return PFK_OK;
+}
+
+const char *pfk_eri_batch_last_error(const pfk_eri_batch *b) { return b ? b->err.c_str() : g_last_error.c_str(); }
+
+pfk_status pfk_eri_batch_set_quartets(pfk_eri_batch *ctx, const int *quartets, long long n, int *cls, int *ncomp)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (!quartets || n <= 0) return ctx->fail(PFK_ERR_INVALID, "no quartets");
+    const int npairs = (int)ctx->pair_pc.size();
+    int c0 = -1;
+    std::vector<uint2> q;
+    try {
+        q.resize((size_t)n);
+    } catch (const std::bad_alloc &) {
+        return ctx->fail(PFK_ERR_NOMEM, "host allocation failed");
+    }
+    for (long long t = 0; t < n; ++t) {
+        const int x = quartets[2 * t], y = quartets[2 * t + 1];
+        if (x < 0 || y < 0 || x >= npairs || y >= npairs)
+            return ctx->fail(PFK_ERR_INVALID, "quartet " + std::to_string(t) + " names a pair out of range");
+        const int px = ctx->pair_pc[x], py = ctx->pair_pc[y];
+        if (px < py)
+            return ctx->fail(PFK_ERR_INVALID, "quartet " + std::to_string(t) +
+                                                  ": the bra pair's class must not be below the ket pair's");
+        const int c = quartet_class(px, py);
+        if (c0 < 0) c0 = c;
+        if (c != c0)
+            return ctx->fail(PFK_ERR_INVALID, "quartet " + std::to_string(t) + " is of another class than quartet 0");
+        q[(size_t)t] = make_uint2((unsigned)x, (unsigned)y);
+    }
+    cudaSetDevice(ctx->device);
+    PFK_CK(ctx->d_quart.alloc((size_t)n));
+    PFK_CK(cudaMemcpyAsync(ctx->d_quart.p, q.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, ctx->stream));
+    PFK_CK(cudaStreamSynchronize(ctx->stream));
+    ctx->nq = n;
+    ctx->cls = c0;
+    int x = 0;
+    while ((x + 1) * (x + 2) / 2 <= c0) ++x;
+    const int y = c0 - x * (x + 1) / 2;
+    if (cls) *cls = c0;
+    if (ncomp) *ncomp = ncart(pc_la(x)) * ncart(pc_lb(x)) * ncart(pc_la(y)) * ncart(pc_lb(y));
+    return PFK_OK;
+}
+
+pfk_status pfk_eri_batch_run(pfk_eri_batch *ctx, long long first, long long count, int engine, int precision,
+                             double *d_out, void *stream)
+{
+    if (!ctx) return PFK_ERR_STATE;
+    if (ctx->cls < 0) return ctx->fail(PFK_ERR_STATE, "no quartets set");
+    if (!d_out) return ctx->fail(PFK_ERR_INVALID, "output is null");
+    if (first < 0 || count <= 0 || first + count > ctx->nq) return ctx->fail(PFK_ERR_INVALID, "quartet range out of bounds");
+    if (engine != PFK_ENGINE_OS && engine != PFK_ENGINE_RYS)
+        return ctx->fail(PFK_ERR_INVALID, "engine must be PFK_ENGINE_OS or PFK_ENGINE_RYS");
+    if (precision != PFK_PREC_FP64 && precision != PFK_PREC_MIXED)
+        return ctx->fail(PFK_ERR_INVALID, "precision must be PFK_PREC_FP64 or PFK_PREC_MIXED");
+    if (engine == PFK_ENGINE_OS && quartet_class_L(ctx->cls) > kOSMaxL)
+        return ctx->fail(PFK_ERR_UNSUPPORTED, "no Obara-Saika kernel above LA+LB+LC+LD = 4 (engine os runs Rys there)");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    JKArgs a{};
+    a.pairs = ctx->d_pairs.p;
+    a.prims = ctx->d_prims.p;
+    a.blk_out = d_out;
+    a.tol = 0.0;
+    a.ptol = 0.0;
+    a.nb = 0;
+    a.qstride = 1;
+    a.qoffset = 0;
+    const int flags = (engine == PFK_ENGINE_OS ? kLaunchOS : 0) | (precision == PFK_PREC_MIXED ? kLaunchFP32 : 0);
+    g_class_launchers[ctx->cls](ctx->d_quart.p + first, count, a, 1, flags, st);
+    PFK_CK(cudaGetLastError());
+    return PFK_OK;
+}
+
+}  // extern "C"
+
+namespace pfk {
+int ctx_device(const pfk_ctx *ctx) { return ctx->device; }
+pfk_status ctx_fail(pfk_ctx *ctx, pfk_status s, const std::string &msg) { return ctx->fail(s, msg); }
+}  // namespace pfk

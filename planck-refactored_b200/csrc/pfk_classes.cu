@@ -41,24 +41,32 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int flag
         else if (fp32) eri_reg_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
         else eri_reg_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
     } else if constexpr (SS::OK) {
+        using SF = SplitShape<LA, LB, LC, LD, float>;
         if (n < 0) {  // configure the current device (shared-memory opt-in)
             cudaFuncSetAttribute(eri_split_kernel<LA, LB, LC, LD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::SMEM);
             cudaFuncSetAttribute(eri_split_kernel<LA, LB, LC, LD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::SMEM);
+            cudaFuncSetAttribute(eri_split_kernel<LA, LB, LC, LD, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SF::SMEM);
             return;
         }
         if (n == 0) return;
         const long long grid = (n + SS::TEAMS - 1) / SS::TEAMS;
         if (nk == 2) eri_split_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, SS::SMEM, st>>>(q, n, a);
+        else if (fp32) eri_split_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, SF::SMEM, st>>>(q, n, a);
         else eri_split_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, SS::SMEM, st>>>(q, n, a);
     } else {
+        using TF = TeamShape<LA, LB, LC, LD, float>;
         if (n < 0) {
             cudaFuncSetAttribute(eri_team_kernel<LA, LB, LC, LD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
             cudaFuncSetAttribute(eri_team_kernel<LA, LB, LC, LD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
+            cudaFuncSetAttribute(eri_team_kernel<LA, LB, LC, LD, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TF::SMEM);
             return;
         }
         if (n == 0) return;
         const long long grid = (n + TS::TEAMS - 1) / TS::TEAMS;
         if (nk == 2) eri_team_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);
+        else if (fp32) eri_team_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, TF::SMEM, st>>>(q, n, a);
         else eri_team_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);
     }
 }

@@ -104,10 +104,15 @@ struct JKArgs {
     const double *__restrict__ Pj;     // density for J
     const double *__restrict__ Pk0;    // densities for K (Pk1 used when NK == 2)
     const double *__restrict__ Pk1;
-    double *Jacc;                       // nb x nb accumulators (unsymmetrised)
-    double *Kacc0;
-    double *Kacc1;
+    // nb x nb fixed-point accumulators (unsymmetrised), two 64-bit words
+    // per element (fx_add); the sums do not depend on the order of the adds
+    unsigned long long *Jacc;
+    unsigned long long *Kacc0;
+    unsigned long long *Kacc1;
     double *eri_out;                    // dense tensor mode (nb^4) when non-null
+    // block mode when non-null: list entry t writes its normalised Cartesian
+    // block, unscreened, to blk_out[t * N ...] (no digestion, no tensor)
+    double *blk_out;
     double tol;
     int nb;
     // this launch evaluates quartets[t * qstride + qoffset], t < nq (one
@@ -285,6 +290,41 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
     p.zeta = x0.x; p.inv_zeta = x0.y; p.Px = x1.x; p.Py = x1.y; p.Pz = x2.x;
     p.PAx = x2.y; p.PAy = x3.x; p.PAz = x3.y; p.Kz = x4.x; p.qp = x4.y;
     return p;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic accumulation.  Every J/K contribution v is rounded to a
+// multiple of 2^-60 and added as an integer, split over two 64-bit words of
+// the element: hi counts units of 2^-28, lo (|lo| <= 2^31 per add) units of
+// 2^-60.  Integer addition is associative, so the accumulated value is the
+// same whatever order the threads, warps, streams and kernels add in, and a
+// build is bitwise reproducible (FP64 atomics are not: their rounding
+// depends on arrival order).  Range: |sum| < 2^34 per element; lo holds up
+// to 2^32 adds per element without overflow.  Resolution: 2^-61 rounding
+// per add, below the last bit of any FP64 value above 2^-8.
+// ---------------------------------------------------------------------------
+using FxWord = unsigned long long;
+constexpr double kFxHiScale = 268435456.0;            // 2^28
+constexpr double kFxLoScale = 4294967296.0;           // 2^32
+constexpr double kFxHiUnit = 1.0 / 268435456.0;       // 2^-28
+constexpr double kFxLoUnit = kFxHiUnit / 4294967296.0;  // 2^-60
+
+__device__ __forceinline__ void fx_add(FxWord *acc, size_t idx, double v)
+{
+    const double x = v * kFxHiScale;            // exact (power-of-two scale)
+    const double h = rint(x);
+    const long long lo = __double2ll_rn((x - h) * kFxLoScale);   // x - h is exact, |x - h| <= 1/2
+    if (h != 0.0) atomicAdd(acc + 2 * idx, (FxWord)__double2ll_rn(h));
+    if (lo != 0) atomicAdd(acc + 2 * idx + 1, (FxWord)lo);
+}
+
+// Value of an accumulated (hi, lo) word pair: lo's multiples of 2^32 move
+// into hi, so both parts convert to double exactly and one rounding remains.
+__host__ __device__ __forceinline__ double fx_value(long long hi, long long lo)
+{
+    const long long rem = lo & 0xffffffffLL;    // in [0, 2^32)
+    const long long carry = (lo - rem) / 4294967296LL;
+    return (double)(hi + carry) * kFxHiUnit + (double)rem * kFxLoUnit;
 }
 
 // Contribution of one canonical AO quartet to the J/K accumulators:

@@ -25,9 +25,9 @@ __host__ __device__ constexpr int quartet_class_L(int c)
     return pc_la(x) + pc_lb(x) + pc_la(y) + pc_lb(y);
 }
 
-// Launch flags.  kLaunchFP32 asks for the FP32-arithmetic variant where the
-// class has one (register-path and Obara-Saika classes with nk == 1; the
-// others run FP64).  kLaunchOS asks for the Obara-Saika kernel, which exists
+// Launch flags.  kLaunchFP32 asks for the FP32-arithmetic variant (every
+// kernel family has one for nk == 1; builds with two exchange densities run
+// FP64).  kLaunchOS asks for the Obara-Saika kernel, which exists
 // for classes with LA+LB+LC+LD <= kOSMaxL; the other classes run Rys.
 // kLaunchDense picks the Obara-Saika kernel compiled for 4 blocks of 128
 // per SM (single exchange density only).
@@ -42,6 +42,11 @@ using ClassLauncher = void (*)(const uint2 *quartets, long long n, const JKArgs 
 // units (each compiled for a range of classes).  A launcher called with
 // n < 0 only configures the current device for its kernels.
 extern ClassLauncher g_class_launchers[kQuartetClasses];
+
+// Context internals for the other units: its CUDA device, and recording a
+// failure message (returns s).
+int ctx_device(const pfk_ctx *ctx);
+pfk_status ctx_fail(pfk_ctx *ctx, pfk_status s, const std::string &msg);
 
 // One-electron integrals S, T, V of a validated basis on `device` (pfk_onee.cu);
 // on failure `what` names the step.

@@ -91,15 +91,16 @@ __device__ __forceinline__ double quartet_weight(bool same_ab, bool same_cd, boo
 //   K(i,k) += sum_jl v Pk(j,l)    K(j,k) += sum_il v Pk(i,l)
 //   K(i,l) += sum_jk v Pk(j,k)    K(j,l) += sum_ik v Pk(i,k)
 // (J = 2 (Jacc + Jacc^T) and K = Kacc + Kacc^T afterwards.)
-// warp_bra: every lane of the (full) warp digests a quartet with this same
-// bra block, so the J(i,j) sums are first added across the warp and one lane
-// issues each atomic instead of 32 lanes hitting the same address.
+// lead >= 0: every live lane of the warp digests a quartet of this same bra
+// block (the others hold zero blocks), so the J(i,j) sums are first added
+// across the warp and lane `lead` (the first live lane) issues each add
+// instead of 32 lanes hitting the same address; lead < 0: each lane adds.
 // SKIP: blocks the caller has already added (kSkipJij, kSkipJkl, kSkipKjk,
 // kSkipKjl bits).
 constexpr int kSkipJij = 1, kSkipJkl = 2, kSkipKjk = 4, kSkipKjl = 8;
 template <int NA, int NB, int NC, int ND, int NK, int SKIP = 0, typename V>
 __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0, int l0, const JKArgs &args,
-                                              bool warp_bra = false)
+                                              int lead = -1)
 {
     const int nb = args.nb;
 #define PFK_V(ia, ib, ic, id) double(v[(((ia) * NB + (ib)) * NC + (ic)) * ND + (id)])
@@ -118,12 +119,12 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                 for (int ic = 0; ic < NC; ++ic)
 #pragma unroll
                     for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ic * ND + id];
-                if (warp_bra) {
+                if (lead >= 0) {
 #pragma unroll
                     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if ((threadIdx.x & 31) == 0) atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+                    if ((int)(threadIdx.x & 31) == lead) fx_add(args.Jacc, (size_t)(i0 + ia) * nb + j0 + ib, s);
                 } else {
-                    atomicAdd(args.Jacc + (size_t)(i0 + ia) * nb + j0 + ib, s);
+                    fx_add(args.Jacc, (size_t)(i0 + ia) * nb + j0 + ib, s);
                 }
             }
     }
@@ -143,12 +144,12 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                 for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
                     for (int ib = 0; ib < NB; ++ib) s += PFK_V(ia, ib, ic, id) * p[ia * NB + ib];
-                atomicAdd(args.Jacc + (size_t)(k0 + ic) * nb + l0 + id, s);
+                fx_add(args.Jacc, (size_t)(k0 + ic) * nb + l0 + id, s);
             }
     }
 #pragma unroll
     for (int m = 0; m < NK; ++m) {
-        double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+        FxWord *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
         const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
         if (!Kacc) continue;
         asm volatile("" ::: "memory");
@@ -167,7 +168,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                     for (int ib = 0; ib < NB; ++ib)
 #pragma unroll
                         for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ib * ND + id];
-                    atomicAdd(Kacc + (size_t)(i0 + ia) * nb + k0 + ic, s);
+                    fx_add(Kacc, (size_t)(i0 + ia) * nb + k0 + ic, s);
                 }
         }
         asm volatile("" ::: "memory");
@@ -186,7 +187,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                     for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
                         for (int id = 0; id < ND; ++id) s += PFK_V(ia, ib, ic, id) * p[ia * ND + id];
-                    atomicAdd(Kacc + (size_t)(j0 + ib) * nb + k0 + ic, s);
+                    fx_add(Kacc, (size_t)(j0 + ib) * nb + k0 + ic, s);
                 }
         }
         asm volatile("" ::: "memory");
@@ -205,7 +206,7 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                     for (int ib = 0; ib < NB; ++ib)
 #pragma unroll
                         for (int ic = 0; ic < NC; ++ic) s += PFK_V(ia, ib, ic, id) * p[ib * NC + ic];
-                    atomicAdd(Kacc + (size_t)(i0 + ia) * nb + l0 + id, s);
+                    fx_add(Kacc, (size_t)(i0 + ia) * nb + l0 + id, s);
                 }
         }
         asm volatile("" ::: "memory");
@@ -224,28 +225,64 @@ __device__ __forceinline__ void digest_blocks(const V *v, int i0, int j0, int k0
                     for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
                         for (int ic = 0; ic < NC; ++ic) s += PFK_V(ia, ib, ic, id) * p[ia * NC + ic];
-                    atomicAdd(Kacc + (size_t)(j0 + ib) * nb + l0 + id, s);
+                    fx_add(Kacc, (size_t)(j0 + ib) * nb + l0 + id, s);
                 }
         }
     }
 #undef PFK_V
 }
 
+// The first live lane when every live lane of the warp digests a quartet of
+// the same bra pair (the J(i,j) sums can then be added across the warp
+// first), else -1.  Every lane of the warp calls it, in kernels where one
+// thread owns a quartet and no sub-warp barrier precedes it (lanes without a
+// quartet pass live = false and carry a zero block), so the answer depends
+// only on the lists, never on which lanes happen to be converged -- part of
+// what keeps a build bitwise reproducible.
+__device__ __forceinline__ int warp_bra_lead(bool live, unsigned bra)
+{
+    const unsigned lv = __ballot_sync(0xffffffffu, live);
+    if (lv == 0u) return -1;
+    const int lead = __ffs(lv) - 1;
+    const unsigned lead_bra = __shfl_sync(0xffffffffu, bra, lead);
+    return __all_sync(0xffffffffu, !live || bra == lead_bra) ? lead : -1;
+}
+
 // Weights (duplicate components, AO-level screening), component norms and
 // J/K digestion of a contracted Cartesian block acc[((ia*NB+ib)*NC+ic)*ND+id]
-// of one shell quartet; in dense-tensor mode the block is scattered instead.
+// of one shell quartet (list entry t); in dense-tensor mode the block is
+// scattered instead, in block mode written out.  Every lane of the warp calls
+// it; lanes with live = false hold a zero block (their digestion adds
+// nothing) and write nothing in the tensor and block modes.
 template <int LA, int LB, int LC, int LD, int NK, typename R>
 __device__ __forceinline__ void finish_block(R *acc, const uint2 qd, const PairInfo &pb, const PairInfo &pk,
-                                             const JKArgs &args)
+                                             const JKArgs &args, bool live, long long t)
 {
     using S = ClassShape<LA, LB, LC, LD>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
+    if (args.blk_out) {
+        if (!live) return;
+        double *o = args.blk_out + (size_t)t * S::N;
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                    for (int id = 0; id < ND; ++id) {
+                        const int c = ((ia * NB + ib) * NC + ic) * ND + id;
+                        o[c] = double(acc[c]) * S::norm(ia, ib, ic, id);
+                    }
+        return;
+    }
     const int nb = args.nb;
     const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
     const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
     const bool check = pb.qmin * pk.qmin < args.tol;
 
     if (args.eri_out) {
+        if (!live) return;
 #pragma unroll
         for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
@@ -278,10 +315,9 @@ __device__ __forceinline__ void finish_block(R *acc, const uint2 qd, const PairI
                                                      args.Qao, nb, i0 + ia, j0 + ib, k0 + ic, l0 + id, args.tol);
                     acc[c] = acc[c] * R(sw * S::norm(ia, ib, ic, id));
                 }
-    // lanes of a full warp usually share the bra pair (lists are bra-major)
-    const unsigned act = __activemask();
-    const bool warp_bra = act == 0xffffffffu && __all_sync(act, __shfl_sync(act, qd.x, 0) == qd.x);
-    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args, warp_bra);
+    // lanes of a warp usually share the bra pair (lists are bra-major)
+    const int lead = warp_bra_lead(live, qd.x);
+    digest_blocks<NA, NB, NC, ND, NK>(acc, i0, j0, k0, l0, args, lead);
 }
 
 // ---------------------------------------------------------------------------
@@ -298,11 +334,15 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
     using S = ClassShape<LA, LB, LC, LD>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nq) return;
-    const uint2 qd = quartets[t * args.qstride + args.qoffset];
+    // Lanes past the end of the list, or whose quartet the density screen
+    // drops, stay with an empty primitive loop and a zero block (see
+    // finish_block); a warp with no quartet at all leaves.
+    const bool in_list = t < nq;
+    if (!__any_sync(0xffffffffu, in_list)) return;
+    const uint2 qd = quartets[(in_list ? t : nq - 1) * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
-    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
+    const bool live = in_list && !density_negligible(pb, pk, args);
 
     R acc[NA * NB * NC * ND];
 #pragma unroll
@@ -311,7 +351,8 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
     const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
-    for (int jp = 0; jp < pk.nprim; ++jp) {
+    const int nket = live ? pk.nprim : 0;
+    for (int jp = 0; jp < nket; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
         if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
@@ -349,21 +390,21 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
         }
     }
 
-    finish_block<LA, LB, LC, LD, NK, R>(acc, qd, pb, pk, args);
+    finish_block<LA, LB, LC, LD, NK, R>(acc, qd, pb, pk, args, live, t);
 }
 
 // ---------------------------------------------------------------------------
 // Team path (TEAM = 8: four quartets per warp; TEAM = 32: one warp per
 // quartet; TEAM = 128: the whole block per quartet).
 // ---------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R = double>
 struct TeamShape {
     using S = ClassShape<LA, LB, LC, LD>;
     static constexpr int TEAM = S::N <= 400 ? 8 : S::N <= 1300 ? 32 : 128;
     static constexpr int TEAMS = 128 / TEAM;
     static constexpr int KPT = (S::N + TEAM - 1) / TEAM;
-    static constexpr int TABLE = S::NR * 3 * S::NI;          // doubles per team
-    static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
+    static constexpr int TABLE = S::NR * 3 * S::NI;          // R values per team
+    static constexpr size_t SMEM = sizeof(R) * TABLE * TEAMS;
 };
 
 template <int TEAM>
@@ -373,14 +414,18 @@ __device__ __forceinline__ void team_sync(unsigned mask)
     else __syncthreads();
 }
 
-template <int LA, int LB, int LC, int LD, int NK>
+// R: the arithmetic type of the axis tables, the products and the
+// contraction (double, or float for the FP32 list); roots, weights and the
+// per-primitive scalars stay FP64, the digestion FP64 with fixed-point sums.
+template <int LA, int LB, int LC, int LD, int NK, typename R = double>
 __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
 {
     using S = ClassShape<LA, LB, LC, LD>;
-    using TS = TeamShape<LA, LB, LC, LD>;
+    using TS = TeamShape<LA, LB, LC, LD, R>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR, NI = S::NI;
     constexpr int TEAM = TS::TEAM, KPT = TS::KPT;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char pfk_dyn_smem[];
+    R *smem = reinterpret_cast<R *>(pfk_dyn_smem);
     const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
     const long long t = (long long)blockIdx.x * TS::TEAMS + team;
     // Teams within a warp synchronise only their own lanes, so a team may
@@ -388,7 +433,7 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
     if (t >= nq) return;
     const unsigned mask = TEAM >= 32 ? 0xffffffffu
                                      : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
-    double *g = smem + team * TS::TABLE;   // g[r][axis][NI]
+    R *g = smem + team * TS::TABLE;   // g[r][axis][NI]
 
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
@@ -396,10 +441,10 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
     if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
 
     int off[KPT];
-    double acc[KPT];
+    R acc[KPT];
 #pragma unroll
     for (int k = 0; k < KPT; ++k) {
-        acc[k] = 0.0;
+        acc[k] = R(0);
         const int c = lane + k * TEAM;
         if (c < S::N) {
             const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
@@ -433,13 +478,14 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
                 if (axis == 0) { C00 = p.PAx + ur * s.WPx; D00 = q.PAx + ur * s.WQx; AB = pb.ABx; CD = pk.ABx; scale = wr * s.pref; }
                 else if (axis == 1) { C00 = p.PAy + ur * s.WPy; D00 = q.PAy + ur * s.WQy; AB = pb.ABy; CD = pk.ABy; }
                 else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
-                axis_table<LA, LB, LC, LD, double>(C00, D00, B00, B10, B01, AB, CD, scale, g + (r * 3 + axis) * NI);
+                axis_table<LA, LB, LC, LD, R>(R(C00), R(D00), R(B00), R(B10), R(B01), R(AB), R(CD), R(scale),
+                                              g + (r * 3 + axis) * NI);
             }
             team_sync<TEAM>(mask);
 #pragma unroll
             for (int k = 0; k < KPT; ++k) {
                 const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
-                double a = acc[k];
+                R a = acc[k];
 #pragma unroll
                 for (int r = 0; r < NR; ++r)
                     a += g[(r * 3 + 0) * NI + ox] * g[(r * 3 + 1) * NI + oy] * g[(r * 3 + 2) * NI + oz];
@@ -449,6 +495,17 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
         }
     }
 
+    if (args.blk_out) {
+#pragma unroll
+        for (int k = 0; k < KPT; ++k) {
+            const int c = lane + k * TEAM;
+            if (c >= S::N) continue;
+            const int id = c % ND, ic = (c / ND) % NC, ib = (c / (ND * NC)) % NB, ia = c / (ND * NC * NB);
+            args.blk_out[(size_t)t * S::N + c] =
+                double(acc[k]) * cart_norm(LA, ia) * cart_norm(LB, ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+        }
+        return;
+    }
     const int nb = args.nb;
     const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
     const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
@@ -462,22 +519,23 @@ __global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__
         const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao, nb,
                                          i, j, kk, l, args.tol);
         if (sw == 0.0) continue;
-        const double v = acc[k] * sw * cart_norm(LA, ia) * cart_norm(LB, ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+        const double v =
+            double(acc[k]) * sw * cart_norm(LA, ia) * cart_norm(LB, ib) * cart_norm(LC, ic) * cart_norm(LD, id);
         if (args.eri_out) {
             scatter8(args.eri_out, nb, i, j, kk, l, v / sw);
             continue;
         }
-        atomicAdd(args.Jacc + (size_t)i * nb + j, v * __ldg(args.Pj + (size_t)kk * nb + l));
-        atomicAdd(args.Jacc + (size_t)kk * nb + l, v * __ldg(args.Pj + (size_t)i * nb + j));
+        fx_add(args.Jacc, (size_t)i * nb + j, v * __ldg(args.Pj + (size_t)kk * nb + l));
+        fx_add(args.Jacc, (size_t)kk * nb + l, v * __ldg(args.Pj + (size_t)i * nb + j));
 #pragma unroll
         for (int m = 0; m < NK; ++m) {
-            double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+            FxWord *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
             const double *__restrict__ Pk = m == 0 ? args.Pk0 : args.Pk1;
             if (!Kacc) continue;
-            atomicAdd(Kacc + (size_t)i * nb + kk, v * __ldg(Pk + (size_t)j * nb + l));
-            atomicAdd(Kacc + (size_t)j * nb + kk, v * __ldg(Pk + (size_t)i * nb + l));
-            atomicAdd(Kacc + (size_t)i * nb + l, v * __ldg(Pk + (size_t)j * nb + kk));
-            atomicAdd(Kacc + (size_t)j * nb + l, v * __ldg(Pk + (size_t)i * nb + kk));
+            fx_add(Kacc, (size_t)i * nb + kk, v * __ldg(Pk + (size_t)j * nb + l));
+            fx_add(Kacc, (size_t)j * nb + kk, v * __ldg(Pk + (size_t)i * nb + l));
+            fx_add(Kacc, (size_t)i * nb + l, v * __ldg(Pk + (size_t)j * nb + kk));
+            fx_add(Kacc, (size_t)j * nb + l, v * __ldg(Pk + (size_t)i * nb + kk));
         }
     }
 }
@@ -585,7 +643,7 @@ namespace pfk {
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int pow2ceil(int x) { return x <= 1 ? 1 : 2 * pow2ceil((x + 1) / 2); }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R = double>
 struct SplitShape {
     using S = ClassShape<LA, LB, LC, LD>;
     static constexpr int LEVEL = (S::NB * S::NC * S::ND <= 64) ? 1 : 2;
@@ -601,15 +659,21 @@ struct SplitShape {
     static constexpr int BST = LEVEL == 2 ? (LC + 1) * (LD + 1) + ((LC + 1) * (LD + 1) + 1) % 2 : (LC + 1) * (LD + 1);
     static constexpr int AST = LEVEL == 1 ? (LB + 1) * BST + ((LB + 1) * BST + 1) % 2 : (LB + 1) * BST;
     static constexpr int NIP = (LA + 1) * AST;                 // padded table per (root, axis)
-    static constexpr int TABLE = S::NR * 3 * NIP + (S::NR * 3 * NIP + 1) % 2;
-    static constexpr size_t SMEM = sizeof(double) * TABLE * TEAMS;
+    // R values per team: an odd number of 8-byte words, so the teams of a
+    // warp start on different bank pairs and every team's table (and the
+    // FP64 reduction staged in it) is 8-byte aligned
+    static constexpr int RAW = S::NR * 3 * NIP;
+    static constexpr int TABLE = sizeof(R) == 8 ? RAW + (RAW + 1) % 2
+                                                : 2 * ((RAW + 1) / 2 + ((RAW + 1) / 2 + 1) % 2);
+    static constexpr size_t SMEM = sizeof(R) * TABLE * TEAMS;
     // team reduction of the blocks every owner adds to the same elements of
     // (LEVEL 1: J(k,l), K(j,k), K(j,l)), staged in the team's table after the
     // primitive loop: REDV partial sums per owner per exchange density
     static constexpr int REDV1 = S::NC * S::ND, REDVK = S::NB * S::NC + S::NB * S::ND;
     template <int NK>
     __host__ __device__ static constexpr int redv() { return REDV1 + NK * REDVK; }
-    static constexpr bool TEAMRED = LEVEL == 1 && TEAM <= 32 && (REDV1 + 2 * REDVK) * GROUP <= TABLE;
+    static constexpr bool TEAMRED =
+        LEVEL == 1 && TEAM <= 32 && (REDV1 + 2 * REDVK) * GROUP * 8 <= TABLE * (int)sizeof(R);
     static constexpr bool OK = TEAM <= 128 && M <= 64;
 };
 
@@ -642,20 +706,28 @@ __device__ __forceinline__ int cart_l_axis(int i, int axis)
     return axis == 0 ? cart_lx(L, i) : axis == 1 ? cart_ly(L, i) : cart_lz(L, i);
 }
 
-template <int LA, int LB, int LC, int LD, int NK>
+// R: the arithmetic type of the shared tables, the slices, the products and
+// the contraction (double, or float for the FP32 list of quartets whose
+// Schwarz bound is below the FP32 threshold); roots, weights and the
+// per-primitive scalars stay FP64, and so does the digestion.
+template <int LA, int LB, int LC, int LD, int NK, typename R = double>
 __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
 {
     using S = ClassShape<LA, LB, LC, LD>;
-    using SS = SplitShape<LA, LB, LC, LD>;
+    using SS = SplitShape<LA, LB, LC, LD, R>;
     constexpr int NB = S::NB, NC = S::NC, ND = S::ND, NR = S::NR;
     constexpr int TEAM = SS::TEAM, LEVEL = SS::LEVEL, NBT = SS::NBT, SB = SS::SB, M = SS::M;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char pfk_dyn_smem[];
+    R *smem = reinterpret_cast<R *>(pfk_dyn_smem);
     const int team = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
     const long long t = (long long)blockIdx.x * SS::TEAMS + team;
-    if (t >= nq) return;   // whole teams leave together; barriers are per team
+    // Whole teams leave together; every barrier below is per team.  No
+    // full-warp intrinsic follows: the teams of a warp run different
+    // primitive loops, each synchronising only its own lanes.
+    if (t >= nq) return;
     const unsigned mask = TEAM >= 32 ? 0xffffffffu
                                      : (((1u << TEAM) - 1u) << ((threadIdx.x & 31) / TEAM * TEAM));
-    double *g = smem + team * SS::TABLE;   // g[r][axis][NIP]
+    R *g = smem + team * SS::TABLE;   // g[r][axis][NIP]
 
     const uint2 qd = quartets[t * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
@@ -673,9 +745,9 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
         base[x] = LEVEL == 1 ? la * SS::AST : la * SS::AST + cart_l_axis<LB>(ib0, x) * SS::BST;
     }
 
-    double acc[M];
+    R acc[M];
 #pragma unroll
-    for (int c = 0; c < M; ++c) acc[c] = 0.0;
+    for (int c = 0; c < M; ++c) acc[c] = R(0);
 
     // ket primitives outer: a warp's lanes usually share the bra pair, so the
     // inner loads of bra primitives are broadcasts
@@ -698,14 +770,14 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                 if (axis == 0) { C00 = p.PAx + ur * s.WPx; D00 = q.PAx + ur * s.WQx; AB = pb.ABx; CD = pk.ABx; scale = wr * s.pref; }
                 else if (axis == 1) { C00 = p.PAy + ur * s.WPy; D00 = q.PAy + ur * s.WQy; AB = pb.ABy; CD = pk.ABy; }
                 else { C00 = p.PAz + ur * s.WPz; D00 = q.PAz + ur * s.WQz; AB = pb.ABz; CD = pk.ABz; }
-                axis_table<LA, LB, LC, LD, double, SS::BST, SS::AST>(C00, D00, B00, B10, B01, AB, CD, scale,
-                                                                       g + (r * 3 + axis) * SS::NIP);
+                axis_table<LA, LB, LC, LD, R, SS::BST, SS::AST>(R(C00), R(D00), R(B00), R(B10), R(B01), R(AB),
+                                                                  R(CD), R(scale), g + (r * 3 + axis) * SS::NIP);
             }
             split_sync<TEAM>(mask, team);
             if (owner) {
 #pragma unroll
                 for (int r = 0; r < NR; ++r) {
-                    double tx[SB], ty[SB], tz[SB];
+                    R tx[SB], ty[SB], tz[SB];
 #pragma unroll
                     for (int e = 0; e < SB; ++e) {
                         tx[e] = g[(r * 3 + 0) * SS::NIP + base[0] + e];
@@ -738,13 +810,28 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
     }
     // ---- digestion of this thread's components: A index ia, B indices
     // ib0 .. ib0 + NBT - 1, all C and D.  Non-owner lanes hold a zero block
-    // (ia = 0) and take part only in the J(i,j) reduction across teams. ----
+    // (ia = 0) and take part only in the team reduction. ----
     const int nb = args.nb;
     const int i0 = pb.bf_a, j0 = pb.bf_b, k0 = pk.bf_a, l0 = pk.bf_b;
     const bool same_ab = (i0 == j0), same_cd = (k0 == l0), same_bk = (qd.x == qd.y);
     const bool check = pb.qmin * pk.qmin < args.tol;
     const int i = i0 + ia;
 
+    if (args.blk_out) {
+        if (!owner) return;
+#pragma unroll
+        for (int bl = 0; bl < NBT; ++bl)
+#pragma unroll
+            for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+                for (int id = 0; id < ND; ++id) {
+                    const int ib = ib0 + bl;
+                    const double nrm = cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+                    args.blk_out[(size_t)t * S::N + ((ia * NB + ib) * NC + ic) * ND + id] =
+                        double(acc[(bl * NC + ic) * ND + id]) * nrm;
+                }
+        return;
+    }
     if (args.eri_out) {
         if (!owner) return;
 #pragma unroll
@@ -758,7 +845,7 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                                                      nb, i, j0 + ib, k0 + ic, l0 + id, args.tol);
                     if (sw != 0.0) {
                         const double nrm = cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
-                        scatter8(args.eri_out, nb, i, j0 + ib, k0 + ic, l0 + id, acc[(bl * NC + ic) * ND + id] * nrm);
+                        scatter8(args.eri_out, nb, i, j0 + ib, k0 + ic, l0 + id, double(acc[(bl * NC + ic) * ND + id]) * nrm);
                     }
                 }
         return;
@@ -774,15 +861,14 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                 const double sw = quartet_weight(same_ab, same_cd, same_bk, ia, ib, ic, id, NB, ND, check, args.Qao, nb,
                                                  i, j0 + ib, k0 + ic, l0 + id, args.tol);
                 acc[(bl * NC + ic) * ND + id] *=
-                    sw * cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id);
+                    R(sw * cart_norm_rt<LA>(ia) * cart_norm_rt<LB>(ib) * cart_norm(LC, ic) * cart_norm(LD, id));
             }
-    // J(i, j0+ib0+bl): the teams of a warp usually share the bra pair, and a
-    // lane's (ia, ib0) depends only on its place in the team, so lanes TEAM
-    // apart add their sums before one team's owners issue the atomics.
+    // J(i, j0+ib0+bl): each owner adds its sums.  (A sum across the teams of
+    // a warp would need a full-warp shuffle right after loops in which the
+    // teams run different trip counts and synchronise only their own lanes;
+    // measured on the GPU, that read lanes' registers before their teams had
+    // written them.)
     {
-        const unsigned act = __activemask();
-        const bool warp_bra = TEAM < 32 && act == 0xffffffffu &&
-                              __all_sync(act, __shfl_sync(act, qd.x, 0) == qd.x);
         double p[NC * ND];
 #pragma unroll
         for (int ic = 0; ic < NC; ++ic)
@@ -794,14 +880,8 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
 #pragma unroll
             for (int ic = 0; ic < NC; ++ic)
 #pragma unroll
-                for (int id = 0; id < ND; ++id) sj += acc[(bl * NC + ic) * ND + id] * p[ic * ND + id];
-            if (warp_bra) {
-#pragma unroll
-                for (int o = TEAM; o < 32; o <<= 1) sj += __shfl_xor_sync(0xffffffffu, sj, o);
-                if (owner && (threadIdx.x & 31) < TEAM) atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, sj);
-            } else if (owner) {
-                atomicAdd(args.Jacc + (size_t)i * nb + j0 + ib0 + bl, sj);
-            }
+                for (int id = 0; id < ND; ++id) sj += double(acc[(bl * NC + ic) * ND + id]) * p[ic * ND + id];
+            if (owner) fx_add(args.Jacc, (size_t)i * nb + j0 + ib0 + bl, sj);
         }
     }
     if constexpr (SS::TEAMRED) {
@@ -809,7 +889,7 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
         // team's (now unused) table; the team then adds them up and one lane
         // per element issues the atomic
         constexpr int V = SS::template redv<NK>();
-        double *red = g;
+        double *red = reinterpret_cast<double *>(g);   // 8-byte aligned (SplitShape::TABLE)
         split_sync<TEAM>(mask, team);
         if (owner) {
             {
@@ -822,7 +902,7 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                     for (int id = 0; id < ND; ++id) {
                         double sj = 0.0;
 #pragma unroll
-                        for (int bl = 0; bl < NB; ++bl) sj += acc[(bl * NC + ic) * ND + id] * pij[bl];
+                        for (int bl = 0; bl < NB; ++bl) sj += double(acc[(bl * NC + ic) * ND + id]) * pij[bl];
                         red[gi * V + ic * ND + id] = sj;
                     }
             }
@@ -842,14 +922,14 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
                     for (int ic = 0; ic < NC; ++ic) {
                         double sk = 0.0;
 #pragma unroll
-                        for (int id = 0; id < ND; ++id) sk += acc[(bl * NC + ic) * ND + id] * pil[id];
+                        for (int id = 0; id < ND; ++id) sk += double(acc[(bl * NC + ic) * ND + id]) * pil[id];
                         r[bl * NC + ic] = sk;                              // K(j,k)
                     }
 #pragma unroll
                     for (int id = 0; id < ND; ++id) {
                         double sk = 0.0;
 #pragma unroll
-                        for (int ic = 0; ic < NC; ++ic) sk += acc[(bl * NC + ic) * ND + id] * pik[ic];
+                        for (int ic = 0; ic < NC; ++ic) sk += double(acc[(bl * NC + ic) * ND + id]) * pik[ic];
                         r[NB * NC + bl * ND + id] = sk;                    // K(j,l)
                     }
                 }
@@ -860,13 +940,13 @@ __global__ void __launch_bounds__(128, 3) eri_split_kernel(const uint2 *__restri
             double sum = 0.0;
             for (int o = 0; o < SS::GROUP; ++o) sum += red[o * V + e];
             if (e < SS::REDV1) {
-                atomicAdd(args.Jacc + (size_t)(k0 + e / ND) * nb + l0 + e % ND, sum);
+                fx_add(args.Jacc, (size_t)(k0 + e / ND) * nb + l0 + e % ND, sum);
             } else {
                 const int m = (e - SS::REDV1) / SS::REDVK, f = (e - SS::REDV1) % SS::REDVK;
-                double *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
+                FxWord *Kacc = m == 0 ? args.Kacc0 : args.Kacc1;
                 if (!Kacc) continue;
-                if (f < NB * NC) atomicAdd(Kacc + (size_t)(j0 + f / NC) * nb + k0 + f % NC, sum);
-                else atomicAdd(Kacc + (size_t)(j0 + (f - NB * NC) / ND) * nb + l0 + (f - NB * NC) % ND, sum);
+                if (f < NB * NC) fx_add(Kacc, (size_t)(j0 + f / NC) * nb + k0 + f % NC, sum);
+                else fx_add(Kacc, (size_t)(j0 + (f - NB * NC) / ND) * nb + l0 + (f - NB * NC) % ND, sum);
             }
         }
     }

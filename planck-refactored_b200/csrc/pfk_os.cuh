@@ -344,11 +344,14 @@ __global__ void __launch_bounds__(128, MINB) eri_os_kernel(const uint2 *__restri
     using O = OSShape<LA, LB, LC, LD>;
     constexpr int L = O::L;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nq) return;
-    const uint2 qd = quartets[t * args.qstride + args.qoffset];
+    // lanes without a quartet stay with an empty primitive loop and a zero
+    // block (finish_block needs the whole warp); a warp with none leaves
+    const bool in_list = t < nq;
+    if (!__any_sync(0xffffffffu, in_list)) return;
+    const uint2 qd = quartets[(in_list ? t : nq - 1) * args.qstride + args.qoffset];
     const PairInfo pb = args.pairs[qd.x];
     const PairInfo pk = args.pairs[qd.y];
-    if (density_negligible(pb, pk, args)) return;   // whole quartet (team-uniform)
+    const bool live = in_list && !density_negligible(pb, pk, args);
 
     R acc[O::NACC];
 #pragma unroll
@@ -358,7 +361,8 @@ __global__ void __launch_bounds__(128, MINB) eri_os_kernel(const uint2 *__restri
     // ahead of the current one was measured slower: its registers cost more
     // occupancy than the latency it hides.
     const double qb0 = pb.nprim ? __ldg(&args.prims[pb.prim_off].qp) : 0.0;   // largest bra qp
-    for (int jp = 0; jp < pk.nprim; ++jp) {
+    const int nket = live ? pk.nprim : 0;
+    for (int jp = 0; jp < nket; ++jp) {
         const PrimPair q = load_prim(args.prims, pk.prim_off + jp);
         if (q.qp * qb0 < args.ptol) break;   // kets sorted by qp
         for (int ip = 0; ip < pb.nprim; ++ip) {
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(128, MINB) eri_os_kernel(const uint2 *__restri
     const R AB[3] = {R(pb.ABx), R(pb.ABy), R(pb.ABz)};
     const R CD[3] = {R(pk.ABx), R(pk.ABy), R(pk.ABz)};
     os_hrr<LA, LB, LC, LD, R>(acc, AB, CD, blk);
-    finish_block<LA, LB, LC, LD, NK, R>(blk, qd, pb, pk, args);
+    finish_block<LA, LB, LC, LD, NK, R>(blk, qd, pb, pk, args, live, t);
 }
 
 }  // namespace pfk

@@ -217,8 +217,17 @@ cudaError_t census(const uint2 *q, long long nq, const PairInfo *pairs, const in
 // ---------------------------------------------------------------------------
 // Finishing kernels (O(nb^2))
 // ---------------------------------------------------------------------------
+// A + A^T of a fixed-point accumulator (fx_add) at (i, j), summed as
+// integers (exact) before the one conversion to double.
+__device__ __forceinline__ double fx_sym(const FxWord *__restrict__ A, size_t ij, size_t ji)
+{
+    const long long hi = (long long)(A[2 * ij] + A[2 * ji]);
+    const long long lo = (long long)(A[2 * ij + 1] + A[2 * ji + 1]);
+    return fx_value(hi, lo);
+}
+
 // out = cj * 2 (J + J^T) + ck * (K + K^T)   (either accumulator may be null)
-__global__ void combine_kernel(const double *__restrict__ J, const double *__restrict__ K, double cj, double ck,
+__global__ void combine_kernel(const FxWord *__restrict__ J, const FxWord *__restrict__ K, double cj, double ck,
                                double *out, int nb)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -226,8 +235,8 @@ __global__ void combine_kernel(const double *__restrict__ J, const double *__res
     const int i = (int)(t / nb), j = (int)(t % nb);
     const size_t ij = (size_t)i * nb + j, ji = (size_t)j * nb + i;
     double v = 0.0;
-    if (J) v += cj * 2.0 * (J[ij] + J[ji]);
-    if (K) v += ck * (K[ij] + K[ji]);
+    if (J) v += cj * 2.0 * fx_sym(J, ij, ji);
+    if (K) v += ck * fx_sym(K, ij, ji);
     out[ij] = v;
 }
 
@@ -237,7 +246,7 @@ __global__ void add_kernel(const double *__restrict__ a, const double *__restric
     if (t < n) out[t] = a[t] + b[t];
 }
 
-cudaError_t combine(const double *J, const double *K, double cj, double ck, double *out, int nb, cudaStream_t st)
+cudaError_t combine(const FxWord *J, const FxWord *K, double cj, double ck, double *out, int nb, cudaStream_t st)
 {
     const long long n = (long long)nb * nb;
     combine_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, K, cj, ck, out, nb);

@@ -18,7 +18,9 @@ cudaError_t fill_quartets(const int *idX, int nX, const int *idY, int diag, cons
 cudaError_t census(const uint2 *q, long long nq, const PairInfo *pairs, const int *pair_la, const int *pair_lb,
                    const double *Qao, int nb, double tol, unsigned long long *counters, int *out, long long cap,
                    cudaStream_t st);
-cudaError_t combine(const double *J, const double *K, double cj, double ck, double *out, int nb, cudaStream_t st);
+// out = cj * 2 (J + J^T) + ck * (K + K^T) from fixed-point accumulators
+// (2 nb^2 words each; either may be null).
+cudaError_t combine(const FxWord *J, const FxWord *K, double cj, double ck, double *out, int nb, cudaStream_t st);
 cudaError_t add(const double *a, const double *b, double *out, long long n, cudaStream_t st);
 cudaError_t bra_work(const int *idX, int nX, int diag, const long long *cnt_hi, const long long *cnt_lo,
                      const long long *kprefY, const PairInfo *pairs, long long *work_hi, long long *work_lo,

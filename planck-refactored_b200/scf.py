@@ -300,8 +300,15 @@ class System:
         return self._incr
 
     def run(self, P0=None, incremental=False, linalg="host", **kw):
-        """RHF to convergence; linalg="device" runs rhf_device (the loop's
-        linear algebra on the GPU) instead of rhf."""
+        """RHF to convergence.  linalg="host": rhf() (numpy linear algebra);
+        "gpu": the whole loop behind the C ABI (pfk_scf_rhf: DIIS and
+        diagonalisation on the device, no Python per iteration), with the
+        difference-density builds when incremental is set; "device": the torch
+        loop rhf_device."""
+        if linalg == "gpu":
+            G0 = kw.pop("G0", None)
+            return self.engine.scf_rhf(self.H, self.S, self.enuc, self.nocc, P0=P0, G0=G0,
+                                       incremental=self.incremental_engine() if incremental else None, **kw)
         if linalg == "device":
             if incremental:
                 raise ValueError("the device loop has no difference-density builds")

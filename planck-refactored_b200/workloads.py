@@ -195,3 +195,57 @@ def random_shells(nshell, lmax=3, seed=11, box=10.0):
         norm.extend(nrm)
     return {"L": np.array(L, dtype=np.int32), "nprim": np.array(nprim, dtype=np.int32),
             "center": np.array(center), "expo": np.array(expo), "coef": np.array(coef), "norm": np.array(norm)}
+
+
+def _normalize_many(L, expo, raw):
+    """basis.normalize over many shells of one angular momentum and one
+    contraction depth (rows of expo / raw), with the same operation order,
+    so every row equals the scalar routine's result."""
+    from . import basis
+    pi = np.pi
+    prefactor = 2.0 ** (2.0 * L + 1.5) / pi ** 1.5
+    norm = np.sqrt(expo ** (L + 1.5) * prefactor)
+    k = expo.shape[1]
+    total = np.zeros(expo.shape[0])
+    for j in range(k):
+        for i in range(k):
+            sij = (pi ** 1.5 / 2.0 ** L) / (expo[:, i] + expo[:, j]) ** (L + 1.5)
+            total += raw[:, i] * raw[:, j] * norm[:, i] * norm[:, j] * sij
+    del basis
+    return raw * (1.0 / np.sqrt(total))[:, None], norm
+
+
+def eri_class_quartets(la, lb, lc, ld, n, seed=0, box=10.0):
+    """The ERI class microbenchmark's inputs for class (la lb|lc ld):
+    n independent shell quartets, each of four fresh shells with centres
+    uniform in a `box` Angstrom cube, contraction depth uniform in 1..6,
+    exponents log-uniform in [0.05, 1e4] and coefficients uniform in (0, 1],
+    normalised as the reference does (basis.cpp:39-75).  Shells 4t..4t+3
+    belong to quartet t; pair 2t is (4t, 4t+1), pair 2t+1 is (4t+2, 4t+3).
+    Requires la >= lb, lc >= ld and (la, lb) >= (lc, ld) in pair-class order.
+    Returns (shells, pairs (2n x 2), quartets (n x 2))."""
+    from . import basis
+    rng = np.random.default_rng([seed, la, lb, lc, ld])
+    ns = 4 * n
+    Ls = np.tile(np.array([la, lb, lc, ld], dtype=np.int32), n)
+    depth = rng.integers(1, 7, size=ns).astype(np.int32)
+    center = rng.uniform(0.0, box, size=(ns, 3)) * basis.ANGSTROM_TO_BOHR
+    E = np.exp(rng.uniform(np.log(0.05), np.log(1e4), size=(ns, 6)))
+    # coefficients in (0, 1]: 1 - U[0, 1) never gives 0
+    Rw = 1.0 - rng.uniform(0.0, 1.0, size=(ns, 6))
+    coef = np.zeros((ns, 6))
+    norm = np.zeros((ns, 6))
+    for L in sorted(set(int(x) for x in (la, lb, lc, ld))):
+        for k in range(1, 7):
+            rows = np.nonzero((Ls == L) & (depth == k))[0]
+            if len(rows) == 0:
+                continue
+            c, nm = _normalize_many(L, E[rows, :k], Rw[rows, :k])
+            coef[rows, :k] = c
+            norm[rows, :k] = nm
+    mask = np.arange(6)[None, :] < depth[:, None]
+    shells = {"L": Ls, "nprim": depth, "center": center, "expo": E[mask], "coef": coef[mask],
+              "norm": norm[mask]}
+    pairs = np.arange(ns, dtype=np.int32).reshape(-1, 2)
+    quartets = np.arange(2 * n, dtype=np.int32).reshape(-1, 2)
+    return shells, pairs, quartets
