@@ -140,7 +140,9 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 
-pfk_status validate(const pfk_basis_desc *b, std::string &why)
+// Basis checks before any device work.  check_nbasis: contexts index basis
+// functions with 16 bits in the quartet codes (ERI batches do not).
+pfk_status validate(const pfk_basis_desc *b, std::string &why, bool check_nbasis = true)
 {
     if (!b || b->nshell <= 0 || !b->L || !b->nprim || !b->center || !b->expo || !b->coef || !b->norm) {
         why = "basis descriptor is null or empty";
@@ -173,7 +175,7 @@ pfk_status validate(const pfk_basis_desc *b, std::string &why)
             why = "exponents must be positive and finite; coefficients and norms finite";
             return PFK_ERR_INVALID;
         }
-    if (nb >= 65536) {
+    if (check_nbasis && nb >= 65536) {
         why = "more than 65535 basis functions";
         return PFK_ERR_UNSUPPORTED;
     }
@@ -1618,7 +1620,7 @@ pfk_status pfk_eri_batch_create(const pfk_basis_desc *basis, int npairs, const i
     }
     *out = nullptr;
     std::string why;
-    pfk_status vs = validate(basis, why);
+    pfk_status vs = validate(basis, why, false);
     if (vs != PFK_OK) {
         g_last_error = "pfk_eri_batch_create: " + why;
         return vs;
