@@ -56,7 +56,8 @@ typedef enum {
 typedef enum { PFK_ENGINE_OS = 0, PFK_ENGINE_RYS = 1, PFK_ENGINE_AUTO = 2 } pfk_engine;
 
 /* FP64 everywhere, or FP32 for quartets whose Schwarz bound is below
- * fp32_bound (roots/weights, Fock accumulation stay FP64). */
+ * fp32_bound (Boys values, roots/weights, Fock accumulation stay FP64).
+ * Classes with an f shell stay FP64 in either mode. */
 typedef enum { PFK_PREC_FP64 = 0, PFK_PREC_MIXED = 1 } pfk_precision;
 
 typedef struct {

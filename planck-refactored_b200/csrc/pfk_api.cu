@@ -303,6 +303,12 @@ void drop_graphs(pfk_ctx *ctx)
     ctx->graphs.clear();
 }
 
+// Pair classes from fs on hold an f shell.  Quartet classes with one keep
+// their whole list in FP64: on the ERI class microbenchmark's random shells
+// the FP32 variants of those classes lose up to 1e-5 (fd|fd) and more
+// (ff|ff), where the s..d classes stay within 1e-7 relative.
+constexpr int kFirstFPairClass = 6;
+
 pfk_status build_lists(pfk_ctx *ctx)
 {
     const double bound = ctx->precision == PFK_PREC_MIXED ? ctx->fp32_bound : 0.0;
@@ -329,8 +335,8 @@ pfk_status build_lists(pfk_ctx *ctx)
             ctx->q_cnt[cls] = ctx->q32_cnt[cls] = 0;
             ctx->prim_cnt[cls] = ctx->prim32_cnt[cls] = 0;
             if (nX == 0 || nY == 0) continue;
-            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
-                                  cnt_lo.p, ctx->stream));
+            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol,
+                                  x >= kFirstFPairClass ? 0.0 : bound, cnt_hi.p, cnt_lo.p, ctx->stream));
             size_t tb = tmp_bytes;
             PFK_CK(exclusive_scan(cnt_hi.p, off_hi.p, nX, tmp.p, tb, ctx->stream));
             tb = tmp_bytes;
@@ -359,8 +365,8 @@ pfk_status build_lists(pfk_ctx *ctx)
             const int cls = quartet_class(x, y);
             const int nX = (int)ctx->cls_ids[x].size(), nY = (int)ctx->cls_ids[y].size();
             if (nX == 0 || nY == 0 || ctx->q_cnt[cls] + ctx->q32_cnt[cls] == 0) continue;
-            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol, bound, cnt_hi.p,
-                                  cnt_lo.p, ctx->stream));
+            PFK_CK(count_quartets(ctx->d_cls_q[x].p, nX, ctx->d_cls_q[y].p, nY, x == y, ctx->tol,
+                                  x >= kFirstFPairClass ? 0.0 : bound, cnt_hi.p, cnt_lo.p, ctx->stream));
             size_t tb = tmp_bytes;
             PFK_CK(exclusive_scan(cnt_hi.p, off_hi.p, nX, tmp.p, tb, ctx->stream));
             tb = tmp_bytes;
