@@ -29,6 +29,15 @@ cores, timed on a bounded sample of pair rows and extrapolated.
 --impl reference times that CPU path alone (the reference's own direct path
 needs an nb^4 = 3.3 TB tensor at 800 functions and cannot run; the streaming
 restatement computes the same integrals without it).
+
+The default line also carries time_to_energy: whole RHF runs of C40H82 /
+cc-pVDZ through pfk_scf_rhf, the plain all-FP64 path from the
+core-Hamiltonian guess against mixed precision with the learned guess.
+
+Other modes (--mode): eri-classes (the ERI class microbenchmark: every class
+(ss|ss)..(ff|ff) on 2^20 seed-random shell quartets, OS and Rys, FP64 and
+FP32, written as a JSON table with --out), mo (the AO -> MO transform and the
+MP2 energy of (H2O)7), scf (whole SCF runs of one molecule several ways).
 """
 import argparse
 import json
@@ -604,6 +613,100 @@ def eri_classes(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# AO -> MO transform and MP2 (pfk_mo_transform, pfk_rmp2_energy)
+# ---------------------------------------------------------------------------
+def mo_transform(args):
+    """Device AO -> MO transform behind MP2: a seeded water cluster in 6-31G**
+    (7 waters: 175 Cartesian functions, the largest cluster under the
+    180-function limit of the dense tensor), the MP2 block (C_occ C_vir |
+    C_occ C_vir) of its converged RHF.  Per phase, the device time from CUDA
+    events inside the call: the AO tensor (class kernels in tensor mode), the
+    four quarter-transform GEMMs (FP64, cuBLAS) against the FP64 FMA peak
+    measured in the same run, and the copy of the block to the host; then the
+    RMP2 energy summed on the host from that block and on the device
+    (pfk_rmp2_energy, the block never leaving HBM)."""
+    P = _pfk()
+    sysm = P.scf.System(P.workloads.water_cluster(args.waters, seed=SEED), "6-31g**", P.basis.load_library())
+    r = sysm.run()
+    nb, no = sysm.H.shape[0], sysm.nocc
+    nv = nb - no
+    C = r["C"]
+    eng = sysm.engine
+    eng.mo_transform(C[:, :no], C[:, no:], C[:, :no], C[:, no:])   # warm-up (BLAS handle, kernels)
+    times = []
+    for _ in range(args.steps):
+        eng.mo_transform(C[:, :no], C[:, no:], C[:, :no], C[:, no:])
+        times.append(eng.mo_transform_times())
+    t = min(times, key=lambda x: x[1])
+    flops = 2.0 * (no * nb ** 4 + no * nv * nb ** 3 + no * nv * no * nb ** 2 + no * nv * no * nv * nb)
+    fp64_peak, _ = P.measure_fma_peak(0)
+    e2 = P.mp2.rmp2(eng, C, r["eps"], no)
+    dev = []
+    for _ in range(args.steps):
+        e_dev = eng.rmp2_energy(C, r["eps"], no)
+        dev.append(eng.mo_transform_times())
+    td = min(dev, key=lambda x: x[1])
+    sysm.close()
+    out = {"workload": f"(H2O){args.waters} 6-31G** ({nb} bf), MP2 block (occ vir|occ vir), nocc {no}, nvir {nv}",
+           "ao_tensor_ms": t[0], "ao_tensor_GBps_written": nb ** 4 * 8 / t[0] / 1e6,
+           "gemm_ms": t[1], "gemm_flops": flops, "gemm_tflops": flops / t[1] / 1e9,
+           "fp64_fma_peak_tflops": fp64_peak, "gemm_frac_of_fp64_peak": flops / t[1] / 1e9 / fp64_peak,
+           "copy_out_ms": t[2], "mo_block_MB": no * nv * no * nv * 8 / 1e6,
+           "rhf_energy": r["energy"], "rmp2_corr": e2,
+           "rmp2_on_device": {"corr": e_dev, "ao_tensor_ms": td[0], "gemm_ms": td[1], "sum_ms": td[2],
+                              "total_ms": sum(td), "block_read_GBps": 2 * no * nv * no * nv * 8 / td[2] / 1e6}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Whole SCF runs, several ways
+# ---------------------------------------------------------------------------
+def scf_runs(args):
+    """Time to converged energy of whole RHF runs on the GPU builds, one
+    molecule several ways (--runs): fp64 (all-FP64 builds, the plain GPU
+    path), mixed (FP32 below a Schwarz bound of 1e-8), mixed+dP (with FP32
+    difference-density builds), and fp64+guess / mixed+guess (the learned
+    guess hook).  --linalg picks the loop: host (numpy), gpu (pfk_scf_rhf
+    behind the C ABI) or device (the torch loop).  Molecules: C40H82 /
+    cc-pVDZ (1010 Cartesian functions) and the 32-water cluster / 6-31G**
+    (800)."""
+    P = _pfk()
+    atoms, basis = ((P.workloads.alkane(40, seed=3, noise=0.03), "cc-pvdz") if args.molecule == "c40h82"
+                    else (P.workloads.water_cluster(32, seed=SEED), "6-31g**"))
+    lib = P.basis.load_library()
+    model_path = args.guess_model or os.path.join(
+        REPO, "planck-refactored_b200", "data", "guess_model_ccpvdz.npz" if basis == "cc-pvdz" else
+        "guess_model_631gs.npz")
+    runs = args.runs.split(",") if args.runs else ["fp64", "mixed", "mixed+dP", "fp64+guess", "mixed+guess"]
+    model = P.guess.GuessModel.load(model_path, device=0) if any("guess" in r for r in runs) else None
+    out = {"molecule": args.molecule, "basis": basis, "linalg": args.linalg, "runs": {}}
+    ref = None
+    for label in runs:
+        prec = "mixed" if label.startswith("mixed") else "fp64"
+        t0 = time.perf_counter()
+        sysm = P.scf.System(atoms, basis, lib, precision=prec, fp32_bound=1e-8)
+        t_setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        P0 = G0 = None
+        if "guess" in label:
+            P0, G0, _ = P.guess.choose(model, sysm)
+        kw = {"G0": G0} if args.linalg != "device" else {}
+        r = sysm.run(P0=P0, incremental="dP" in label, linalg=args.linalg, **kw)
+        wall = time.perf_counter() - t0
+        sysm.close()
+        if ref is None:
+            ref = r["energy"]
+        out["runs"][label] = {"energy": r["energy"], "dE_vs_first_run": r["energy"] - ref,
+                              "iterations": r["iterations"], "converged": r["converged"],
+                              "seconds_to_convergence": wall, "setup_seconds": t_setup}
+    if model is not None:
+        model.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -623,8 +726,14 @@ def main():
                     help="streams the class kernels of a build are spread over")
     ap.add_argument("--waters", type=int, default=32,
                     help="cluster size; 32 is the benchmark workload, smaller sizes are for profiling")
-    ap.add_argument("--mode", choices=["fock", "eri-classes"], default="fock",
-                    help="fock: the Fock-build benchmark (default); eri-classes: the ERI class microbenchmark")
+    ap.add_argument("--mode", choices=["fock", "eri-classes", "mo", "scf"], default="fock",
+                    help="fock: the Fock-build benchmark (default); eri-classes: the ERI class microbenchmark; "
+                         "mo: the AO->MO transform and MP2 on (H2O)7; scf: whole SCF runs several ways")
+    ap.add_argument("--molecule", choices=["c40h82", "water32"], default="c40h82", help="scf: the molecule")
+    ap.add_argument("--runs", default="", help="scf: comma-separated subset of fp64,mixed,mixed+dP,fp64+guess,"
+                                               "mixed+guess")
+    ap.add_argument("--linalg", choices=["host", "gpu", "device"], default="gpu", help="scf: the SCF loop")
+    ap.add_argument("--guess-model", default="", help="scf: learned-guess model (default: the shipped one)")
     ap.add_argument("--quartets", type=int, default=1 << 20, help="eri-classes: shell quartets per class")
     ap.add_argument("--classes", default="", help="eri-classes: comma-separated class indices (default: all 55)")
     ap.add_argument("--oracle-quartets", type=int, default=4096, help="eri-classes: oracle subset per class")
@@ -633,6 +742,12 @@ def main():
     args = ap.parse_args()
     if args.mode == "eri-classes":
         return eri_classes(args)
+    if args.mode == "mo":
+        if args.waters == 32:
+            args.waters = 7
+        return mo_transform(args)
+    if args.mode == "scf":
+        return scf_runs(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -4,9 +4,10 @@
 # standard library), plus the C shim in this directory.  The rest of the
 # reference's integral code needs Eigen 3.4 (fetched by its CMake at configure
 # time, absent here), so it is not built; the oracle restates it instead.
-# Usage: oracle/build_ref.sh [reference-root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference-root]
+#        (default: $PLANCK_REFERENCE_ROOT, else /root/reference)
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${PLANCK_REFERENCE_ROOT:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 mkdir -p "$HERE/_ref"
 if [ ! -f "$REF/src/lookup/boys.cpp" ]; then

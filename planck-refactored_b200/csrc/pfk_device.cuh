@@ -293,37 +293,49 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic accumulation.  Every J/K contribution v is rounded to a
-// multiple of 2^-60 and added as an integer, split over two 64-bit words of
-// the element: hi counts units of 2^-28, lo (|lo| <= 2^31 per add) units of
-// 2^-60.  Integer addition is associative, so the accumulated value is the
-// same whatever order the threads, warps, streams and kernels add in, and a
-// build is bitwise reproducible (FP64 atomics are not: their rounding
-// depends on arrival order).  Range: |sum| < 2^34 per element; lo holds up
-// to 2^32 adds per element without overflow.  Resolution: 2^-61 rounding
-// per add, below the last bit of any FP64 value above 2^-8.
+// Deterministic accumulation.  Every J/K contribution v is rounded to the
+// nearest multiple of 2^-60, X = rint(v 2^60), and added as an integer split
+// over two 64-bit words of the element: X = hi 2^36 + lo with |lo| <= 2^35,
+// so contributions below 2^-25 in magnitude touch only lo.  Integer
+// addition is associative, so the accumulated value is the same whatever
+// order the threads, warps, streams and kernels add in, and a build is
+// bitwise reproducible (FP64 atomics are not: their rounding depends on
+// arrival order).  The value is hi_sum 2^-24 + lo_sum 2^-60 whichever way
+// each X was split.  Range: |sum| < 2^29 per element; lo holds 2^28
+// full-size adds per element.  Resolution: 2^-61 rounding per add, below
+// the last bit of any FP64 value above 2^-8.
 // ---------------------------------------------------------------------------
 using FxWord = unsigned long long;
-constexpr double kFxHiScale = 268435456.0;            // 2^28
-constexpr double kFxLoScale = 4294967296.0;           // 2^32
-constexpr double kFxHiUnit = 1.0 / 268435456.0;       // 2^-28
-constexpr double kFxLoUnit = kFxHiUnit / 4294967296.0;  // 2^-60
+constexpr double kFxUnitScale = 1152921504606846976.0;   // 2^60
+constexpr double kFxHiScale = 16777216.0;                 // 2^24: units of hi
+constexpr double kFxLoScale = 68719476736.0;              // 2^36: lo units per hi unit
+constexpr long long kFxSplit = 1LL << 36;
+constexpr double kFxHiUnit = 1.0 / 16777216.0;             // 2^-24
+constexpr double kFxLoUnit = 1.0 / 1152921504606846976.0;  // 2^-60
 
 __device__ __forceinline__ void fx_add(FxWord *acc, size_t idx, double v)
 {
-    const double x = v * kFxHiScale;            // exact (power-of-two scale)
-    const double h = rint(x);
-    const long long lo = __double2ll_rn((x - h) * kFxLoScale);   // x - h is exact, |x - h| <= 1/2
-    if (h != 0.0) atomicAdd(acc + 2 * idx, (FxWord)__double2ll_rn(h));
+    long long hi, lo;
+    if (fabs(v) < 8.0) {   // X = rint(v 2^60) fits in 63 bits: one conversion, integer split
+        const long long X = __double2ll_rn(v * kFxUnitScale);   // exact scale
+        hi = (X + (kFxSplit >> 1)) >> 36;                        // arithmetic shift: floor
+        lo = X - hi * kFxSplit;                                  // in [-2^35, 2^35)
+    } else {               // large v: the same X in two steps (x - rint(x) is exact)
+        const double x = v * kFxHiScale;
+        const double h = rint(x);
+        hi = __double2ll_rn(h);
+        lo = __double2ll_rn((x - h) * kFxLoScale);               // |lo| <= 2^35
+    }
+    if (hi != 0) atomicAdd(acc + 2 * idx, (FxWord)hi);
     if (lo != 0) atomicAdd(acc + 2 * idx + 1, (FxWord)lo);
 }
 
-// Value of an accumulated (hi, lo) word pair: lo's multiples of 2^32 move
+// Value of an accumulated (hi, lo) word pair: lo's multiples of 2^36 move
 // into hi, so both parts convert to double exactly and one rounding remains.
 __host__ __device__ __forceinline__ double fx_value(long long hi, long long lo)
 {
-    const long long rem = lo & 0xffffffffLL;    // in [0, 2^32)
-    const long long carry = (lo - rem) / 4294967296LL;
+    const long long rem = lo & (kFxSplit - 1);   // in [0, 2^36)
+    const long long carry = (lo - rem) / kFxSplit;
     return (double)(hi + carry) * kFxHiUnit + (double)rem * kFxLoUnit;
 }
 

@@ -71,8 +71,10 @@ static __constant__ const BoysSeriesTable kBoysSeries = make_boys_series_table()
 // 1 - e^-T erfcx(sqrt T), so one exponential serves all m) and the upward
 // recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T); its error growth stays
 // below ~10x for m <= 4 at T >= 2 (~2x for m <= 1 at T >= 1; TS = 3 for
-// m = 5, 6).  T >= TA (50, or 60 for M > 4): the large-T limit F_0 =
-// sqrt(pi / 4T), F_{m+1} = (2m+1) F_m / (2T), with no erf or exp.
+// m = 5, 6).  T >= TA: the large-T limit F_0 = sqrt(pi / 4T), F_{m+1} =
+// (2m+1) F_m / (2T), with no erf or exp; TA = 34, 38, 42, 44, 46 for
+// M = 0..4 is where the limit's relative error (the dropped e^-T terms)
+// falls to its own rounding level against 40-digit values, 60 above M = 4.
 // Measured against 40-digit values: max relative error 1e-15 (M <= 1),
 // 8e-15 (M = 4), 2e-14 (M = 6).
 template <int M>
@@ -80,7 +82,7 @@ __device__ __forceinline__ void boys_fm(double T, double *F)
 {
     constexpr double TS = M <= 1 ? 1.0 : M <= 4 ? 2.0 : 3.0;
     constexpr int NT = M <= 1 ? 18 : M <= 4 ? 25 : 32;   // terms: last term < 1e-17 at T = TS
-    constexpr double TA = M <= 4 ? 50.0 : 60.0;           // large-T limit from here on
+    constexpr double TA = M == 0 ? 34.0 : M == 1 ? 38.0 : M == 2 ? 42.0 : M == 3 ? 44.0 : M == 4 ? 46.0 : 60.0;
     if (T < TS) {
         double s = kBoysSeries.c[M][NT - 1];
 #pragma unroll

@@ -1,8 +1,9 @@
 """Regenerate the committed golden fixtures from the reference tree.
 
-Run in a container where the reference is mounted (default /root/reference):
+Run where the reference is mounted (--ref, default $PLANCK_REFERENCE_ROOT or
+/root/reference):
 
-    python tests/golden/make_fixtures.py [--ref /root/reference]
+    python tests/golden/make_fixtures.py [--ref REFERENCE_ROOT]
 
 Writes, next to this script:
   ../../planck-refactored_b200/data/basis_sets.json
@@ -106,7 +107,7 @@ def parse_hfinp(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PLANCK_REFERENCE_ROOT", "/root/reference"))
     args = ap.parse_args()
     ref = args.ref
 
