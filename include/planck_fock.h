@@ -158,8 +158,9 @@ pfk_status pfk_rmp2_energy(pfk_ctx *ctx, const double *C, const double *eps, int
 /* UMP2 correlation energy of a converged UHF (run_ump2,
  * src/post_hf/mp2.cpp:43-143): the alpha-alpha and beta-beta terms
  * 1/4 sum [(ia|jb) - (ib|ja)]^2 / D and the alpha-beta term sum (ia|jb)^2 / D
- * over three device-resident (ov|ov) blocks, each made as by
- * pfk_mo_transform and summed where it was made.  Ca, Cb: host nbasis x
+ * over three device-resident (ov|ov) blocks, transformed as by
+ * pfk_mo_transform from one AO tensor built once, and summed where they were
+ * made.  Ca, Cb: host nbasis x
  * nbasis MO coefficients per spin, column-major, occupied first; eps_a, eps_b
  * their orbital energies.  nbasis <= 180. */
 pfk_status pfk_ump2_energy(pfk_ctx *ctx, const double *Ca, const double *eps_a, const double *Cb, const double *eps_b,

@@ -1016,10 +1016,13 @@ __global__ void __launch_bounds__(256) mp2_sum_kernel(const double *__restrict__
 // result goes to the host buffer `out`, or, with eps1 set (blocks occ, vir,
 // occ, vir; eps1 and eps2 the nbasis orbital energies of the first and the
 // second pair's spin), into the MP2 sum of `mode` in *e_corr without leaving
-// the device.
+// the device.  shared_E: an AO tensor (nbasis^4) kept across calls -- built
+// by the first call that gets it empty, then reused and left intact (the
+// second quarter's result then gets its own buffer instead of overwriting
+// the tensor); null: a tensor of this call only.
 static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C2, int n2, const double *C3, int n3,
                          const double *C4, int n4, double *out, const double *eps1, const double *eps2, int mode,
-                         double *e_corr)
+                         double *e_corr, DevBuf<double> *shared_E = nullptr)
 {
     const int nb = ctx->nb;
     if (n1 < 1 || n2 < 1 || n3 < 1 || n4 < 1 || n1 > nb || n2 > nb || n3 > nb || n4 > nb)
@@ -1032,10 +1035,13 @@ static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C
     }
     if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return ctx->fail(PFK_ERR_CUDA, "cublasSetStream failed");
     const size_t b = nb, b2 = b * b, b3 = b2 * b;
-    // two buffers, allocated before the timed work: the AO tensor E and T1;
-    // T2 (n1 n2 nb^2 <= nb^4) then reuses E, T3 (n1 n2 n3 nb <= n1 nb^3)
-    // reuses T1, and the result (n1 n2 n3 n4 <= n1 n2 nb^2) reuses E
-    DevBuf<double> E, T1, dC[4];
+    // buffers allocated before the timed work: the AO tensor E and T1; T2
+    // (n1 n2 nb^2 <= nb^4) then reuses E (or, with a shared tensor, a buffer
+    // of its own), T3 (n1 n2 n3 nb <= n1 nb^3) reuses T1, and the result
+    // (n1 n2 n3 n4 <= n1 n2 nb^2) reuses T2's buffer
+    DevBuf<double> own_E, T1, T2buf, dC[4];
+    DevBuf<double> &E = shared_E ? *shared_E : own_E;
+    const bool build_E = E.p == nullptr;
     const double *hC[4] = {C1, C2, C3, C4};
     const int nk[4] = {n1, n2, n3, n4};
     for (int k = 0; k < 4; ++k) {
@@ -1048,18 +1054,22 @@ static pfk_status mo_run(pfk_ctx *ctx, const double *C1, int n1, const double *C
         ~EvFree() { for (int k = 0; k < 4; ++k) if (e[k]) cudaEventDestroy(e[k]); }
     } ev_free{ev};
     for (auto &x : ev) PFK_CK(cudaEventCreate(&x));
-    PFK_CK(E.alloc(b2 * b2));
+    if (build_E) PFK_CK(E.alloc(b2 * b2));
     PFK_CK(T1.alloc(b3 * n1));
+    if (shared_E) PFK_CK(T2buf.alloc(b2 * (size_t)n1 * n2));
     PFK_CK(cudaEventRecord(ev[0], st));
-    PFK_CK(cudaMemsetAsync(E.p, 0, sizeof(double) * b2 * b2, st));
-    pfk_status s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, E.p, st, false);
-    if (s != PFK_OK) return s;
+    pfk_status s = PFK_OK;
+    if (build_E) {
+        PFK_CK(cudaMemsetAsync(E.p, 0, sizeof(double) * b2 * b2, st));
+        s = run_classes(ctx, ctx->d_P.p, ctx->d_P.p, nullptr, 1, ctx->d_J.p, nullptr, nullptr, E.p, st, false);
+        if (s != PFK_OK) return s;
+    }
     PFK_CK(cudaEventRecord(ev[1], st));
     const double one = 1.0, zero = 0.0;
     auto ck = [&](cublasStatus_t r, const char *what) {
         return r == CUBLAS_STATUS_SUCCESS ? PFK_OK : ctx->fail(PFK_ERR_CUDA, std::string(what) + " failed");
     };
-    double *T2 = E.p, *T3 = T1.p, *O = E.p;
+    double *T2 = shared_E ? T2buf.p : E.p, *T3 = T1.p, *O = T2;
     s = ck(cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)b3, n1, nb, &one, E.p, (int)b3, dC[0].p, nb, &zero,
                        T1.p, (int)b3),
            "quarter transform 1 (cublasDgemm)");
@@ -1165,11 +1175,13 @@ pfk_status pfk_ump2_energy(pfk_ctx *ctx, const double *Ca, const double *eps_a, 
         return ctx->fail(PFK_ERR_INVALID, "no occupied or virtual orbitals in a spin channel");
     const double *Cav = Ca + (size_t)nb * n_alpha, *Cbv = Cb + (size_t)nb * n_beta;
     double e_aa = 0.0, e_bb = 0.0, e_ab = 0.0;
-    pfk_status s = mo_run(ctx, Ca, n_alpha, Cav, nva, Ca, n_alpha, Cav, nva, nullptr, eps_a, eps_a, kMp2Same, &e_aa);
+    DevBuf<double> E;   // the AO tensor, built by the first transform and shared by all three
+    pfk_status s =
+        mo_run(ctx, Ca, n_alpha, Cav, nva, Ca, n_alpha, Cav, nva, nullptr, eps_a, eps_a, kMp2Same, &e_aa, &E);
     if (s == PFK_OK)
-        s = mo_run(ctx, Cb, n_beta, Cbv, nvb, Cb, n_beta, Cbv, nvb, nullptr, eps_b, eps_b, kMp2Same, &e_bb);
+        s = mo_run(ctx, Cb, n_beta, Cbv, nvb, Cb, n_beta, Cbv, nvb, nullptr, eps_b, eps_b, kMp2Same, &e_bb, &E);
     if (s == PFK_OK)
-        s = mo_run(ctx, Ca, n_alpha, Cav, nva, Cb, n_beta, Cbv, nvb, nullptr, eps_a, eps_b, kMp2Opp, &e_ab);
+        s = mo_run(ctx, Ca, n_alpha, Cav, nva, Cb, n_beta, Cbv, nvb, nullptr, eps_a, eps_b, kMp2Opp, &e_ab, &E);
     if (s == PFK_OK) *e_corr = e_aa + e_bb + e_ab;
     return s;
 }
