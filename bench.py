@@ -580,8 +580,9 @@ def eri_classes(args):
                         take = min(cnt, ncheck - first)
                         keep[v].append(bufs[v][:take * nc].view(take, nc).cpu().numpy())
         batch.close()
-        blocks = {f"{v[0]}_{v[1]}": np.concatenate(keep[v]) for v in keep}
-        n_or, orc = _oracle_block_check(shells, ncheck, blocks, args.oracle_budget)
+        blocks = {f"{v[0]}_{v[1]}": np.concatenate(keep[v]) for v in keep if keep[v]}
+        n_or, orc = (_oracle_block_check(shells, ncheck, blocks, args.oracle_budget) if ncheck > 0 else
+                     (0, {f"{v[0]}_{v[1]}": {"max_rel_err": None, "frac_within_1e-10": None} for v in keep}))
         for v in variants:
             peak = fp64_peak if v[1] == "fp64" else fp32_peak
             rate = flops / (ms[v] * 1e-3) / 1e12
