@@ -472,7 +472,15 @@ def ours_arm(args):
             line["cpu_baseline"] = {k: v for k, v in cpu_fock_rate(shells, budget_s=args.cpu_budget).items()
                                     if k != "est_seconds_per_build"}
         if world == 1 and not args.no_scf:
-            line["time_to_energy"] = time_to_energy(local)
+            # in a child process that never imports torch, as a C++ host would
+            # run it: torch ships its own cuBLAS and cuSOLVER, and once loaded
+            # they are the copies this library's calls bind to
+            env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--mode", "time-to-energy"],
+                               capture_output=True, text=True, env=env)
+            tte = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            line["time_to_energy"] = json.loads(tte[-1]) if r.returncode == 0 and tte else \
+                {"error": (r.stderr or r.stdout)[-500:]}
         result = line
         print(json.dumps(line), flush=True)
     eng.close()
@@ -727,7 +735,7 @@ def main():
                     help="streams the class kernels of a build are spread over")
     ap.add_argument("--waters", type=int, default=32,
                     help="cluster size; 32 is the benchmark workload, smaller sizes are for profiling")
-    ap.add_argument("--mode", choices=["fock", "eri-classes", "mo", "scf"], default="fock",
+    ap.add_argument("--mode", choices=["fock", "eri-classes", "mo", "scf", "time-to-energy"], default="fock",
                     help="fock: the Fock-build benchmark (default); eri-classes: the ERI class microbenchmark; "
                          "mo: the AO->MO transform and MP2 on (H2O)7; scf: whole SCF runs several ways")
     ap.add_argument("--molecule", choices=["c40h82", "water32"], default="c40h82", help="scf: the molecule")
@@ -749,6 +757,9 @@ def main():
         return mo_transform(args)
     if args.mode == "scf":
         return scf_runs(args)
+    if args.mode == "time-to-energy":
+        print(json.dumps(time_to_energy(0)), flush=True)
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -316,7 +316,7 @@ constexpr double kFxLoUnit = 1.0 / 1152921504606846976.0;  // 2^-60
 __device__ __forceinline__ void fx_add(FxWord *acc, size_t idx, double v)
 {
     long long hi, lo;
-    if (fabs(v) < 8.0) {   // X = rint(v 2^60) fits in 63 bits: one conversion, integer split
+    if (fabs(v) < 4.0) {   // X = rint(v 2^60) and X + 2^35 fit in 63 bits: one conversion, integer split
         const long long X = __double2ll_rn(v * kFxUnitScale);   // exact scale
         hi = (X + (kFxSplit >> 1)) >> 36;                        // arithmetic shift: floor
         lo = X - hi * kFxSplit;                                  // in [-2^35, 2^35)

@@ -244,12 +244,22 @@ extern "C" pfk_status pfk_scf_rhf(pfk_ctx *ctx, const double *H, const double *S
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{st};
     Handles h;
+    Dev dv;
+    // the libraries' own choices pinned, so that a run's bits depend only on
+    // its inputs: no atomics in cuBLAS, a fixed cuBLAS workspace (its kernel
+    // choice can depend on the workspace it finds), cuSOLVER's deterministic
+    // mode
+    constexpr size_t kBlasWorkspace = size_t(32) << 20;
+    double *dBlasWs = nullptr;
+    SCF_CK(dv.get(&dBlasWs, kBlasWorkspace / sizeof(double)));
     SCF_BL(cublasCreate(&h.blas));
     SCF_BL(cublasSetStream(h.blas, st));
+    SCF_BL(cublasSetAtomicsMode(h.blas, CUBLAS_ATOMICS_NOT_ALLOWED));
+    SCF_BL(cublasSetWorkspace(h.blas, dBlasWs, kBlasWorkspace));
     SCF_SO(cusolverDnCreate(&h.sol));
     SCF_SO(cusolverDnSetStream(h.sol, st));
+    SCF_SO(cusolverDnSetDeterministicMode(h.sol, CUSOLVER_DETERMINISTIC_RESULTS));
 
-    Dev dv;
     double *dH, *dS, *dX, *dP, *dPb, *dG, *dGd, *dF, *dT1, *dT2, *dE, *dW, *dPart, *dFs, *dEs, *dDP;
     for (double **p : {&dH, &dS, &dX, &dP, &dPb, &dG, &dGd, &dF, &dT1, &dT2, &dE, &dDP}) SCF_CK(dv.get(p, n2));
     SCF_CK(dv.get(&dW, nb));
