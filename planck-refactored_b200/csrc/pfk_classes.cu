@@ -65,9 +65,9 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int flag
         }
         if (n == 0) return;
         const long long grid = (n + TS::TEAMS - 1) / TS::TEAMS;
-        if (nk == 2) eri_team_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);
-        else if (fp32) eri_team_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, TF::SMEM, st>>>(q, n, a);
-        else eri_team_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, TS::SMEM, st>>>(q, n, a);
+        if (nk == 2) eri_team_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, TS::BLOCK, TS::SMEM, st>>>(q, n, a);
+        else if (fp32) eri_team_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, TF::BLOCK, TF::SMEM, st>>>(q, n, a);
+        else eri_team_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, TS::BLOCK, TS::SMEM, st>>>(q, n, a);
     }
 }
 

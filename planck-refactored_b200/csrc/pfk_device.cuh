@@ -301,31 +301,34 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
 // order the threads, warps, streams and kernels add in, and a build is
 // bitwise reproducible (FP64 atomics are not: their rounding depends on
 // arrival order).  The value is hi_sum 2^-24 + lo_sum 2^-60 whichever way
-// each X was split.  Range: |sum| < 2^29 per element; lo holds 2^28
-// full-size adds per element.  Resolution: 2^-61 rounding per add, below
-// the last bit of any FP64 value above 2^-8.
+// each X was split.  Range: |v| < 2^27 per contribution, |sum| < 2^29 per
+// element; lo holds 2^28 full-size adds per element.  Resolution: 2^-61
+// rounding per add, below the last bit of any FP64 value above 2^-8.
+//
+// The split needs no float-to-integer conversion: adding 1.5 2^52 to a
+// double t with |t| < 2^51 leaves a sum whose unit in the last place is 1,
+// so the sum is 1.5 2^52 + rint(t) and its bit pattern minus that of
+// 1.5 2^52 is the integer rint(t).  hi = rint(v 2^24) that way; the
+// remainder r = v 2^24 - hi is exact, and lo = rint(r 2^36) the same way,
+// with one fused multiply-add.  hi 2^36 + lo = rint(v 2^60), because hi 2^36
+// is an even integer and so shifts neither the rounding nor its ties.
 // ---------------------------------------------------------------------------
 using FxWord = unsigned long long;
-constexpr double kFxUnitScale = 1152921504606846976.0;   // 2^60
 constexpr double kFxHiScale = 16777216.0;                 // 2^24: units of hi
 constexpr double kFxLoScale = 68719476736.0;              // 2^36: lo units per hi unit
 constexpr long long kFxSplit = 1LL << 36;
 constexpr double kFxHiUnit = 1.0 / 16777216.0;             // 2^-24
 constexpr double kFxLoUnit = 1.0 / 1152921504606846976.0;  // 2^-60
+constexpr double kFxMagic = 6755399441055744.0;            // 1.5 2^52
 
 __device__ __forceinline__ void fx_add(FxWord *acc, size_t idx, double v)
 {
-    long long hi, lo;
-    if (fabs(v) < 4.0) {   // X = rint(v 2^60) and X + 2^35 fit in 63 bits: one conversion, integer split
-        const long long X = __double2ll_rn(v * kFxUnitScale);   // exact scale
-        hi = (X + (kFxSplit >> 1)) >> 36;                        // arithmetic shift: floor
-        lo = X - hi * kFxSplit;                                  // in [-2^35, 2^35)
-    } else {               // large v: the same X in two steps (x - rint(x) is exact)
-        const double x = v * kFxHiScale;
-        const double h = rint(x);
-        hi = __double2ll_rn(h);
-        lo = __double2ll_rn((x - h) * kFxLoScale);               // |lo| <= 2^35
-    }
+    const double t = v * kFxHiScale;                                           // exact
+    const double a = t + kFxMagic;                                             // 1.5 2^52 + rint(t)
+    const long long hi = __double_as_longlong(a) - __double_as_longlong(kFxMagic);
+    const double r = t - (a - kFxMagic);                                       // exact, |r| <= 1/2
+    const double b = fma(r, kFxLoScale, kFxMagic);                             // 1.5 2^52 + rint(r 2^36)
+    const long long lo = __double_as_longlong(b) - __double_as_longlong(kFxMagic);   // |lo| <= 2^35
     if (hi != 0) atomicAdd(acc + 2 * idx, (FxWord)hi);
     if (lo != 0) atomicAdd(acc + 2 * idx + 1, (FxWord)lo);
 }

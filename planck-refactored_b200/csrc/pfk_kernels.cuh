@@ -397,11 +397,15 @@ __global__ void __launch_bounds__(128) eri_reg_kernel(const uint2 *__restrict__ 
 // Team path (TEAM = 8: four quartets per warp; TEAM = 32: one warp per
 // quartet; TEAM = 128: the whole block per quartet).
 // ---------------------------------------------------------------------------
+// BLOCK threads per block: 128, or 256 for the classes above 4000
+// components ((ff|fd), (ff|ff)), whose 128-thread teams held 63..79
+// accumulators per thread and spilled them.
 template <int LA, int LB, int LC, int LD, typename R = double>
 struct TeamShape {
     using S = ClassShape<LA, LB, LC, LD>;
-    static constexpr int TEAM = S::N <= 400 ? 8 : S::N <= 1300 ? 32 : 128;
-    static constexpr int TEAMS = 128 / TEAM;
+    static constexpr int TEAM = S::N <= 400 ? 8 : S::N <= 1300 ? 32 : S::N <= 4000 ? 128 : 256;
+    static constexpr int BLOCK = TEAM > 128 ? TEAM : 128;
+    static constexpr int TEAMS = BLOCK / TEAM;
     static constexpr int KPT = (S::N + TEAM - 1) / TEAM;
     static constexpr int TABLE = S::NR * 3 * S::NI;          // R values per team
     static constexpr size_t SMEM = sizeof(R) * TABLE * TEAMS;
@@ -418,7 +422,8 @@ __device__ __forceinline__ void team_sync(unsigned mask)
 // contraction (double, or float for the FP32 list); roots, weights and the
 // per-primitive scalars stay FP64, the digestion FP64 with fixed-point sums.
 template <int LA, int LB, int LC, int LD, int NK, typename R = double>
-__global__ void __launch_bounds__(128) eri_team_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
+__global__ void __launch_bounds__(TeamShape<LA, LB, LC, LD, R>::BLOCK) eri_team_kernel(const uint2 *__restrict__ quartets,
+                                                                                  long long nq, JKArgs args)
 {
     using S = ClassShape<LA, LB, LC, LD>;
     using TS = TeamShape<LA, LB, LC, LD, R>;
