@@ -191,6 +191,35 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
+def reference_auto_rys_share(cls):
+    """Share of the Cartesian component quartets of class cls, e.g. "(dp|ps)",
+    that the reference's per-component `engine auto` cost model sends to Rys
+    (rys.cpp:195-220: Rys when its work estimate, 2D-table size times roots
+    plus the transfer and a per-root cost, is below OS's, table size times
+    L + 1 plus the transfer), with the pairs oriented L(A) >= L(B) as this
+    library orients them.  Reported beside the autotuner's per-class choice."""
+    ls = ["spdf".index(ch) for ch in cls if ch in "spdf"]
+
+    def carts(L):
+        return [(L - yz, yz - z, z) for yz in range(L + 1) for z in range(yz + 1)]
+    n = rys = 0
+    for a in carts(ls[0]):
+        for b in carts(ls[1]):
+            for c in carts(ls[2]):
+                for d in carts(ls[3]):
+                    ab = [a[k] + b[k] for k in range(3)]
+                    cd = [c[k] + d[k] for k in range(3)]
+                    L = sum(ab) + sum(cd)
+                    nroots = L // 2 + 1
+                    six = float(np.prod([x + 1 for x in ab + cd]))
+                    hrr = sum(b) + sum(d) + 1
+                    os_work = six * (L + 1) + hrr * six * 0.25
+                    rys_work = six * nroots + hrr * six * 0.20 + 24.0 * nroots
+                    n += 1
+                    rys += rys_work < os_work
+    return rys / n
+
+
 def _traffic_from_profiles(kernel_class):
     """DRAM bytes per launch of the dominant class kernel from the committed
     ncu summary (profiles/ncu_traffic.json), when it covers this class."""
@@ -462,6 +491,8 @@ def ours_arm(args):
                 "classes_shell_quartets": {k: v[0] for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
                 "autotune": None if tuned is None else
                 {"seconds": t_tune, "choice": {k: v[0] for k, v in tuned.items()
+                                               if k in dict(sorted(cls.items(), key=lambda kv: -kv[1][2])[:12])},
+                 "reference_model_rys_share": {k: round(reference_auto_rys_share(k), 3) for k, v in tuned.items()
                                                if k in dict(sorted(cls.items(), key=lambda kv: -kv[1][2])[:12])}},
                 "classes_ms_rys_kernels": None if cls_rys is None else
                 {k: round(cls_rys[k][2], 3) for k, v in sorted(cls.items(), key=lambda kv: -kv[1][2])[:12]},
@@ -599,7 +630,8 @@ def eri_classes(args):
                    "quartets_per_s": n / (ms[v] * 1e-3), "flop_alg_tflops": rate,
                    "frac_of_measured_peak": rate / peak,
                    "peak": "fp64 FMA" if v[1] == "fp64" else "fp32 FMA",
-                   "max_abs_err_vs_rys_fp64": err[v], "max_rel_err_vs_rys_fp64": rel[v]}
+                   "max_abs_err_vs_rys_fp64": err[v], "max_rel_err_vs_rys_fp64": rel[v],
+                   "reference_model_rys_share": round(reference_auto_rys_share(name), 3)}
             if v[1] == "fp64":
                 row["oracle"] = dict(orc[f"{v[0]}_{v[1]}"], quartets=n_or)
             rows.append(row)

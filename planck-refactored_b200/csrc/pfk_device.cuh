@@ -305,13 +305,15 @@ __device__ __forceinline__ PrimPair load_prim(const PrimPair *__restrict__ a, in
 // element; lo holds 2^28 full-size adds per element.  Resolution: 2^-61
 // rounding per add, below the last bit of any FP64 value above 2^-8.
 //
-// The split needs no float-to-integer conversion: adding 1.5 2^52 to a
-// double t with |t| < 2^51 leaves a sum whose unit in the last place is 1,
-// so the sum is 1.5 2^52 + rint(t) and its bit pattern minus that of
-// 1.5 2^52 is the integer rint(t).  hi = rint(v 2^24) that way; the
-// remainder r = v 2^24 - hi is exact, and lo = rint(r 2^36) the same way,
-// with one fused multiply-add.  hi 2^36 + lo = rint(v 2^60), because hi 2^36
-// is an even integer and so shifts neither the rounding nor its ties.
+// The split needs no float-to-integer conversion: a double in [2^52, 2^53)
+// has a unit in the last place of 1, so fma(v, 2^24, 1.5 2^52), rounded
+// once, is 1.5 2^52 + rint(v 2^24) for |v| < 2^27, and its bit pattern minus
+// that of 1.5 2^52 is the integer hi = rint(v 2^24) (1.5 2^52 is even, so
+// ties still go to even).  The remainder r = v 2^24 - hi is exact (one more
+// fma), and lo = rint(r 2^36) comes out the same way.  hi 2^36 + lo =
+// rint(v 2^60), because hi 2^36 is an even integer and so shifts neither the
+// rounding nor its ties.  Zero contributions (empty blocks) add nothing, and
+// hi is added only when it is non-zero.
 // ---------------------------------------------------------------------------
 using FxWord = unsigned long long;
 constexpr double kFxHiScale = 16777216.0;                 // 2^24: units of hi
@@ -323,14 +325,14 @@ constexpr double kFxMagic = 6755399441055744.0;            // 1.5 2^52
 
 __device__ __forceinline__ void fx_add(FxWord *acc, size_t idx, double v)
 {
-    const double t = v * kFxHiScale;                                           // exact
-    const double a = t + kFxMagic;                                             // 1.5 2^52 + rint(t)
-    const long long hi = __double_as_longlong(a) - __double_as_longlong(kFxMagic);
-    const double r = t - (a - kFxMagic);                                       // exact, |r| <= 1/2
-    const double b = fma(r, kFxLoScale, kFxMagic);                             // 1.5 2^52 + rint(r 2^36)
-    const long long lo = __double_as_longlong(b) - __double_as_longlong(kFxMagic);   // |lo| <= 2^35
-    if (hi != 0) atomicAdd(acc + 2 * idx, (FxWord)hi);
-    if (lo != 0) atomicAdd(acc + 2 * idx + 1, (FxWord)lo);
+    if (v == 0.0) return;
+    const double a = fma(v, kFxHiScale, kFxMagic);   // 1.5 2^52 + hi
+    const double h = a - kFxMagic;                   // hi, exact
+    const double r = fma(v, kFxHiScale, -h);         // v 2^24 - hi, exact, |r| <= 1/2
+    const double b = fma(r, kFxLoScale, kFxMagic);   // 1.5 2^52 + lo, |lo| <= 2^35
+    FxWord *p = acc + 2 * idx;
+    if (h != 0.0) atomicAdd(p, (FxWord)(__double_as_longlong(a) - __double_as_longlong(kFxMagic)));
+    atomicAdd(p + 1, (FxWord)(__double_as_longlong(b) - __double_as_longlong(kFxMagic)));
 }
 
 // Value of an accumulated (hi, lo) word pair: lo's multiples of 2^36 move

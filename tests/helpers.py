@@ -37,6 +37,18 @@ def random_shells(*a, **k):
     return pfk().workloads.random_shells(*a, **k)
 
 
+def onee_highprec():
+    """40-digit nuclear-attraction matrix of the random s..f test basis
+    (tests/golden/make_onee_highprec.py): {"V": nb x nb, "coords": nuclei}."""
+    with open(os.path.join(GOLDEN, "onee_highprec.json")) as f:
+        g = json.load(f)
+    nb = g["nbasis"]
+    V = np.zeros((nb, nb))
+    for i, j, v in g["V_upper"]:
+        V[i, j] = V[j, i] = float(v)
+    return {"V": V, "coords": np.array(g["nuclei"]["coords_bohr"])}
+
+
 def random_density(nb, seed=5, scale=0.3):
     rng = np.random.default_rng(seed)
     A = rng.normal(size=(nb, nb)) * scale

@@ -2,11 +2,12 @@
 (GPU tests): forward pass, gradients of one batch, one Adam step, and a
 short training run that must lower the loss.
 
-The device products are BF16 x BF16 with FP32 accumulation and the oracle
-rounds to BF16 at the same points in float64, so the two differ by FP32
-accumulation order and by the rare value that lands on the other side of a
-BF16 rounding boundary: relative error norms below 1e-2 per parameter
-block, and below 1e-4 for the forward output."""
+The device products (tcgen05.mma) are BF16 x BF16 with FP32 accumulation
+and the oracle rounds to BF16 at the same points in float64, so the two
+differ by FP32 accumulation order and by the rare value that lands on the
+other side of a BF16 rounding boundary: relative error norms below 2e-3 per
+parameter block (measured: at most 2.1e-4, on the 112-256-256-232 network),
+and below 1e-4 for the forward output (measured: at most 3.5e-5)."""
 import numpy as np
 import pytest
 
@@ -47,7 +48,7 @@ def test_forward_and_gradients_match_oracle(dims, n):
     for din, dout in zip(dims[:-1], dims[1:]):
         for size in (din * dout, dout):
             a, b = g[o:o + size], go[o:o + size]
-            assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b) + 1e-12
+            assert np.linalg.norm(a - b) <= 2e-3 * np.linalg.norm(b) + 1e-12
             o += size
     net.close()
 

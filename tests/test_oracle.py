@@ -77,3 +77,34 @@ def test_quartet_list_water():
     n, digest, lst = bas.quartet_list(1e-10, Q, want_list=True)
     assert n <= 325 * 326 // 2 and n == len(lst)
     assert np.all(lst[:, 0] <= lst[:, 1]) and np.all(lst[:, 2] <= lst[:, 3])
+
+
+def test_one_electron_against_40_digit_values():
+    """The oracle's V (the reference's os.cpp:294-602) on the random s..f basis
+    of the one-electron GPU test, against 40-digit values
+    (golden/make_onee_highprec.py).  S and T are not in the fixture.  V agrees
+    to 1e-10 relative everywhere except in the two same-shell (f|V|f) blocks,
+    where it is off by up to 7.4e-9: there the recurrences need F_m up to m = 6
+    of tight primitive pairs, and the reference's Boys values (its 15-decimal
+    table and interpolation) carry the error -- the same float64 recurrences
+    with exact Boys values land within 2e-13."""
+    import importlib
+
+    from helpers import onee_highprec
+    P = importlib.import_module("planck-refactored_b200")
+    shells = P.workloads.random_shells(10, lmax=3, seed=31, box=3.0)
+    g = onee_highprec()
+
+    class M:
+        pass
+    mol = M()
+    mol.coords, mol.Z = g["coords"], np.array([1.0, 6.0, 8.0, 7.0])
+    _, _, Vo = oracle.Basis(shells).one_electron(mol)
+    D = np.abs(Vo - g["V"])
+    scale = max(1.0, np.abs(g["V"]).max())
+    L = np.asarray(shells["L"])
+    ao = np.concatenate([[0], np.cumsum((L + 1) * (L + 2) // 2)])
+    sh = np.searchsorted(ao, np.arange(ao[-1]), side="right") - 1
+    bad = np.argwhere(D > 1e-10 * scale)
+    assert all(sh[i] == sh[j] and L[sh[i]] == 3 for i, j in bad)
+    assert D.max() < 1e-8 * scale
