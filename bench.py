@@ -221,16 +221,21 @@ def reference_auto_rys_share(cls):
 
 
 def _traffic_from_profiles(kernel_class):
-    """DRAM bytes per launch of the dominant class kernel from the committed
-    ncu summary (profiles/ncu_traffic.json), when it covers this class."""
+    """(DRAM bytes per launch, where that number comes from) for the dominant
+    class kernel, from the committed ncu summary profiles/ncu_traffic.json
+    when it covers this class: a static estimate from an earlier capture, not
+    a measurement of this run (ncu replays kernels and is never run inside
+    the timed bench)."""
     path = os.path.join(REPO, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
         e = d.get("classes", {}).get(kernel_class)
-        return None if e is None else e.get("dram_bytes_per_full_launch")
+        if e is None:
+            return None, None
+        return e.get("dram_bytes_per_full_launch"), "static estimate, not measured in this run: " + d.get("source", "")
     except (OSError, ValueError):
-        return None
+        return None, None
 
 
 def time_to_energy(device, runs=("fp64", "mixed+guess", "mixed+guess+dP"), model_path=None):
@@ -479,7 +484,8 @@ def ours_arm(args):
                         "d2h_bytes_per_step": d2h, "timing": "wall clock around the blocking C-ABI call"},
                 "roofline": {"bound": "fp64", "kernel": f"eri class {top[0]}", "achieved": top_ach,
                              "peak": fp64_peak, "unit": "TFLOP/s", "frac": top_ach / fp64_peak,
-                             "traffic": _traffic_from_profiles(top[0]),
+                             "traffic": _traffic_from_profiles(top[0])[0],
+                             "traffic_source": _traffic_from_profiles(top[0])[1],
                              "peak_source": "FP64 FMA loop measured in this run (pfk_measure_fma_peak); "
                                             "the driver's peaks file lists HBM and BF16 only",
                              "flops_per_launch": top_flops, "launch_ms": top[1][2]},
@@ -545,6 +551,7 @@ def _oracle_block_check(shells, n_check, blocks, budget_s):
     within = {k: 0 for k in blocks}
     ncomp = next(iter(blocks.values())).shape[1]
     done = 0
+    t_blocks = 0.0
     while done < n_check and time.perf_counter() - t0 < budget_s:
         g = min(group, n_check - done)
         s0, s1 = 4 * done, 4 * (done + g)
@@ -553,13 +560,16 @@ def _oracle_block_check(shells, n_check, blocks, budget_s):
                "norm": shells["norm"][off[s0]:off[s1]]}
         ob = oracle.Basis(sub)
         for k in range(g):
+            tb = time.perf_counter()
             ref = ob.shell_block(4 * k, 4 * k + 1, 4 * k + 2, 4 * k + 3, oracle.RYS)
+            t_blocks += time.perf_counter() - tb
             for name, blk in blocks.items():
                 d = np.abs(blk[done + k] - ref) / np.maximum(1.0, np.abs(ref))
                 worst[name] = max(worst[name], float(d.max()))
                 within[name] += int((d <= 1e-10).sum())
         done += g
-    return done, {k: {"max_rel_err": worst[k], "frac_within_1e-10": within[k] / max(1, done * ncomp)}
+    return done, {k: {"max_rel_err": worst[k], "frac_within_1e-10": within[k] / max(1, done * ncomp),
+                      "cpu_quartets_per_s_1_thread": done / t_blocks if t_blocks > 0 else None}
                   for k in blocks}
 
 
@@ -621,7 +631,8 @@ def eri_classes(args):
         batch.close()
         blocks = {f"{v[0]}_{v[1]}": np.concatenate(keep[v]) for v in keep if keep[v]}
         n_or, orc = (_oracle_block_check(shells, ncheck, blocks, args.oracle_budget) if ncheck > 0 else
-                     (0, {f"{v[0]}_{v[1]}": {"max_rel_err": None, "frac_within_1e-10": None} for v in keep}))
+                     (0, {f"{v[0]}_{v[1]}": {"max_rel_err": None, "frac_within_1e-10": None,
+                                              "cpu_quartets_per_s_1_thread": None} for v in keep}))
         for v in variants:
             peak = fp64_peak if v[1] == "fp64" else fp32_peak
             rate = flops / (ms[v] * 1e-3) / 1e12
@@ -646,7 +657,10 @@ def eri_classes(args):
            "fp64_fma_peak_tflops": fp64_peak, "fp32_fma_peak_tflops": fp32_peak,
            "oracle": "first quartets of each class against the oracle's per-component Rys integrals "
                      f"(up to {args.oracle_quartets} quartets or {args.oracle_budget} s per class); "
-                     "relative to max(1, |v|)",
+                     "relative to max(1, |v|); cpu_quartets_per_s_1_thread is the oracle's rate on those quartets "
+                     "(one host thread, the shell-block calls alone): the reference's per-component contraction "
+                     "(rys.cpp:489-505) restated, the CPU baseline of this table",
+           "host_threads_available": os.cpu_count(),
            "rows": rows}
     if args.out:
         with open(args.out, "w") as f:

@@ -1803,5 +1803,10 @@ pfk_status pfk_eri_batch_run(pfk_eri_batch *ctx, long long first, long long coun
 
 namespace pfk {
 int ctx_device(const pfk_ctx *ctx) { return ctx->device; }
+pfk_status fock_rhf_direct(pfk_ctx *ctx, const double *dP, double *dG, cudaStream_t st)
+{
+    cudaSetDevice(ctx->device);
+    return rhf_sequence(ctx, dP, dG, st);
+}
 pfk_status ctx_fail(pfk_ctx *ctx, pfk_status s, const std::string &msg) { return ctx->fail(s, msg); }
 }  // namespace pfk

@@ -1,7 +1,10 @@
 // pfk_scf.cu -- the RHF loop on the device behind the C ABI (pfk_scf_rhf).
 //
 // The steps of the reference's run_rhf (src/scf/scf.cpp:175-441) with the
-// two-electron part from the context's captured Fock-build graph:
+// two-electron part from the context's Fock build, launched directly on the
+// loop's own stream (no graph capture, so that several loops, one per
+// context, can run at once from host threads; capturing in several threads
+// at once failed with cudaStreamWaitEvent "invalid argument" there):
 //   * symmetric orthogonaliser X = S^-1/2 (scf.cpp:15-20);
 //   * default guess from the eigenvectors of X^T H X (scf.cpp:33-45), or the
 //     caller's density, which enters like a ReadDensity guess
@@ -34,6 +37,11 @@
 #include "pfk_internal.h"
 
 namespace pfk {
+
+// The RHF build G(dP) on stream st launched directly, without capturing a
+// graph (pfk_api.cu; pfk_fock_rhf_device captures one per (dP, dG, stream)).
+pfk_status fock_rhf_direct(pfk_ctx *ctx, const double *dP, double *dG, cudaStream_t st);
+
 namespace {
 
 constexpr int kRedThreads = 256;
@@ -348,7 +356,7 @@ extern "C" pfk_status pfk_scf_rhf(pfk_ctx *ctx, const double *H, const double *S
     } eg{ev0, ev1};
     auto build = [&](pfk_ctx *c, const double *src, double *dst) -> pfk_status {
         SCF_CK(cudaEventRecord(ev0, st));
-        pfk_status s = pfk_fock_rhf_device(c, src, dst, st);
+        pfk_status s = fock_rhf_direct(c, src, dst, st);
         if (s != PFK_OK) return ctx_fail(ctx, s, std::string("pfk_scf_rhf: build: ") + pfk_last_error(c));
         SCF_CK(cudaEventRecord(ev1, st));
         SCF_CK(cudaEventSynchronize(ev1));
