@@ -88,22 +88,29 @@ def cmd_train(args):
     print(json.dumps({"train_seconds": time.perf_counter() - t0, "final_loss": losses}), flush=True)
 
 
-def evaluate(model_path, n, device=0, lo=8, hi=20, log=None):
+def evaluate(model_path, n, device=0, lo=8, hi=20, log=None, linalg="host", batch=1):
+    """Default against learned guess on n held-out conformers.  batch > 1:
+    the molecules go in groups of `batch` SCF runs at once (one context and
+    one device SCF loop per molecule, host threads; linalg "gpu"), the
+    learned guesses of a group predicted one after another (the network is
+    shared); the times are then the groups' wall times."""
     P = _pkg()
     G = P.guess
     lib = P.basis.load_library()
     model = G.GuessModel.load(model_path, device=device)
     basis = model.basis_name
+    if batch > 1:
+        return _evaluate_batched(P, G, lib, model, basis, n, device, lo, hi, log, linalg, batch)
     rows = []
     for i in range(n):
         nc, atoms = conformer(i, lo, hi, 1_000_000)
         sysm = P.scf.System(atoms, basis, lib, device=device)
         t0 = time.perf_counter()
-        r_d = sysm.run()
+        r_d = sysm.run(linalg=linalg)
         t_d = time.perf_counter() - t0
         t0 = time.perf_counter()
         P0, G0, info = G.choose(model, sysm)
-        r_l = sysm.run(P0=P0, G0=G0)
+        r_l = sysm.run(P0=P0, G0=G0, linalg=linalg)
         t_l = time.perf_counter() - t0
         sysm.close()
         # builds: the learned path also pays the default guess's first build
@@ -115,21 +122,58 @@ def evaluate(model_path, n, device=0, lo=8, hi=20, log=None):
         if log and (i + 1) % 64 == 0:
             log(f"evaluated {i + 1}/{n}")
     model.close()
+    return _summary(rows, n, basis, lo, hi)
+
+
+def _summary(rows, n, basis, lo, hi, extra=None):
     it_d = np.array([r["it_default"] for r in rows])
     it_l = np.array([r["it_learned"] for r in rows])
     return {"molecules": n, "basis": basis, "sizes": f"C{lo}-C{hi}",
             "mean_iterations_default": float(it_d.mean()), "mean_iterations_learned": float(it_l.mean()),
             "iterations_ratio": float(it_l.sum() / it_d.sum()),
             "fock_builds_ratio": float(sum(r["builds_learned"] for r in rows) / sum(r["builds_default"] for r in rows)),
-            "seconds_default": float(sum(r["t_default"] for r in rows)),
-            "seconds_learned": float(sum(r["t_learned"] for r in rows)),
+            "seconds_default": float(sum(r["t_default"] or 0.0 for r in rows)),
+            "seconds_learned": float(sum(r["t_learned"] or 0.0 for r in rows)),
             "accepted_fraction": float(np.mean([r["accepted"] for r in rows])),
             "max_abs_dE_Eh": float(max(r["dE"] for r in rows)),
-            "all_converged": bool(all(r["converged"] for r in rows)), "per_molecule": rows}
+            "all_converged": bool(all(r["converged"] for r in rows)), **(extra or {}), "per_molecule": rows}
+
+
+def _evaluate_batched(P, G, lib, model, basis, n, device, lo, hi, log, linalg, batch):
+    from concurrent.futures import ThreadPoolExecutor
+    rows, t_setup, t_def, t_lrn = [], 0.0, 0.0, 0.0
+    with ThreadPoolExecutor(batch) as pool:
+        for g0 in range(0, n, batch):
+            idx = list(range(g0, min(n, g0 + batch)))
+            t0 = time.perf_counter()
+            mols = [conformer(i, lo, hi, 1_000_000) for i in idx]
+            systems = [P.scf.System(atoms, basis, lib, device=device) for _, atoms in mols]
+            t_setup += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            r_d = list(pool.map(lambda s: s.run(linalg=linalg), systems))
+            t_def += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            picks = [G.choose(model, s) for s in systems]
+            r_l = list(pool.map(lambda a: a[0].run(P0=a[1][0], G0=a[1][1], linalg=linalg), zip(systems, picks)))
+            t_lrn += time.perf_counter() - t0
+            for (nc, _), s, rd, rl, pk in zip(mols, systems, r_d, r_l, picks):
+                rows.append({"nc": nc, "nbasis": int(s.H.shape[0]), "it_default": rd["iterations"],
+                             "it_learned": rl["iterations"], "builds_default": rd["iterations"],
+                             "builds_learned": rl["iterations"] + 1, "t_default": None, "t_learned": None,
+                             "accepted": pk[2]["accepted"], "dE": abs(rl["energy"] - rd["energy"]),
+                             "converged": bool(rd["converged"] and rl["converged"])})
+                s.close()
+            if log and len(rows) % 64 == 0:
+                log(f"evaluated {len(rows)}/{n}")
+    model.close()
+    out = _summary(rows, n, basis, lo, hi, {"batch": batch, "linalg": linalg, "setup_seconds": t_setup})
+    out["seconds_default"], out["seconds_learned"] = t_def, t_lrn
+    return out
 
 
 def cmd_evaluate(args):
-    res = evaluate(args.model, args.n, args.device, log=lambda s: print(s, flush=True))
+    res = evaluate(args.model, args.n, args.device, log=lambda s: print(s, flush=True), linalg=args.linalg,
+                   batch=args.batch)
     with open(args.out, "w") as f:
         json.dump(res, f)
     print(json.dumps({k: v for k, v in res.items() if k != "per_molecule"}), flush=True)
@@ -153,6 +197,9 @@ def main():
     e.add_argument("--n", type=int, default=512)
     e.add_argument("--out", default="guess_eval.json")
     e.add_argument("--device", type=int, default=0)
+    e.add_argument("--linalg", default="host", choices=["host", "gpu"],
+                   help="SCF loop: numpy on the host, or pfk_scf_rhf on the device")
+    e.add_argument("--batch", type=int, default=1, help="SCF runs at once (host threads, one context each)")
     args = ap.parse_args()
     {"train": cmd_train, "evaluate": cmd_evaluate}[args.cmd](args)
 
