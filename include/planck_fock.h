@@ -291,7 +291,10 @@ pfk_status pfk_eri_batch_run(pfk_eri_batch *b, long long first, long long count,
  * iteration (the learned-guess hook makes it).  H, S, P0, G0 and the outputs
  * P_out, C_out (MO coefficients, column-major), eps_out are host arrays and
  * may be NULL where optional; the sums are in a fixed order, so a run is
- * bitwise reproducible. */
+ * bitwise reproducible.  The loop runs on a stream of its own, launches its
+ * builds directly (no graph capture) and returns when done, so calls on
+ * different contexts may run at once from several host threads (one
+ * context per thread). */
 typedef struct {
     int max_iter;              /* 0: the reference's limit by basis size */
     double tol_energy;         /* 1e-10 */

@@ -154,6 +154,25 @@ def test_c_abi_scf_loop_matches_reference_regressions(case_id):
         assert abs(r["iterations"] - c["iterations"]) <= 1
 
 
+def test_c_abi_scf_loops_in_threads_repeat_bitwise():
+    """Three device SCF loops (pfk_scf_rhf, one context each) run at once
+    from host threads -- the way guess_train.py evaluate --batch runs the
+    held-out set -- give bitwise the energies, densities and iteration
+    counts of the same loops run one after the other."""
+    from concurrent.futures import ThreadPoolExecutor
+    P = pfk()
+    systems = [P.scf.System(water_cluster(n, seed=11 + n), "6-31g**", basis_library()) for n in (2, 3, 4)]
+    seq = [s.run(linalg="gpu") for s in systems]
+    with ThreadPoolExecutor(3) as pool:
+        par = list(pool.map(lambda s: s.run(linalg="gpu"), systems))
+    for s in systems:
+        s.close()
+    for a, b in zip(seq, par):
+        assert a["converged"] and b["converged"]
+        assert a["energy"] == b["energy"] and a["iterations"] == b["iterations"]
+        assert np.array_equal(a["P"], b["P"])
+
+
 def test_c_abi_scf_loop_matches_host_loop_and_repeats():
     """(H2O)4 / 6-31G**: the C-ABI loop takes the host loop's steps -- the same
     energy at every iteration (1e-9 Eh) while the density steps are above 1e-8
