@@ -223,8 +223,9 @@ pfk_status pfk_set_primitive_tol(pfk_ctx *ctx, double ptol);
 /* Autotuner for engine auto: times every candidate kernel of every class on
  * this context's screened lists (a warm-up pass, then the faster of two timed
  * passes) and keeps the fastest per class for the builds made with engine
- * auto.  Candidates: 0 = Rys, 2 = Obara-Saika, 6 = Obara-Saika compiled for 4
- * blocks of 128 threads per SM; the last two exist for classes with
+ * auto.  Candidates: 0 = Rys, 2 = Obara-Saika, 6 = Obara-Saika compiled for
+ * more blocks of 128 threads per SM (8 for LA+LB+LC+LD <= 1, 6 for 2, 4
+ * above: fewer registers per thread); the last two exist for classes with
  * LA+LB+LC+LD <= 4, the others always run Rys.  Until it runs, engine auto
  * uses the reference's outcome (OS for L <= 4, Rys above).  choice55 (may be
  * NULL) receives the chosen candidate per class, ms55x3 (may be NULL) the

@@ -1230,7 +1230,8 @@ pfk_status pfk_autotune(pfk_ctx *ctx, int *choice55, double *ms55x3)
     if (s != PFK_OK) return s;
     const size_t nb2 = (size_t)ctx->nb * ctx->nb;
     PFK_CK(cudaMemsetAsync(ctx->d_P.p, 0, sizeof(double) * nb2, ctx->stream));   // timing only needs a density
-    // candidates: Rys, Obara-Saika, Obara-Saika at 4 blocks/SM (L <= kOSMaxL only)
+    // candidates: Rys, Obara-Saika, Obara-Saika built for more blocks per SM
+    // (8, 6 or 4 by class; L <= kOSMaxL only)
     const int candidates[3] = {0, kLaunchOS, kLaunchOS | kLaunchDense};
     double t[kQuartetClasses][3] = {};
     const int engine = ctx->engine;

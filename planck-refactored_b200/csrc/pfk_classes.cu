@@ -26,10 +26,17 @@ void launch_class(const uint2 *q, long long n, const JKArgs &a, int nk, int flag
             if (n <= 0) return;
             const long long grid = (n + 127) / 128;
             const bool dense = flags & kLaunchDense;
+            // the denser build: blocks per SM its register cap must allow.  Up
+            // to L = 2 the kernels need at most 104 registers, so 4 blocks would
+            // change nothing; there 8 (L <= 1: 64 registers) and 6 (L = 2: 80)
+            // trade a few spilled values for occupancy.  The autotuner keeps
+            // whichever build is faster on the molecule's lists.
+            constexpr int L = LA + LB + LC + LD;
+            constexpr int MB = L <= 1 ? 8 : L == 2 ? 6 : 4;
             if (nk == 2) eri_os_kernel<LA, LB, LC, LD, 2><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
-            else if (fp32 && dense) eri_os_kernel<LA, LB, LC, LD, 1, float, 4><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else if (fp32 && dense) eri_os_kernel<LA, LB, LC, LD, 1, float, MB><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             else if (fp32) eri_os_kernel<LA, LB, LC, LD, 1, float><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
-            else if (dense) eri_os_kernel<LA, LB, LC, LD, 1, double, 4><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
+            else if (dense) eri_os_kernel<LA, LB, LC, LD, 1, double, MB><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             else eri_os_kernel<LA, LB, LC, LD, 1><<<(unsigned)grid, 128, 0, st>>>(q, n, a);
             return;
         }

@@ -338,8 +338,9 @@ __device__ __forceinline__ void os_hrr(const R *__restrict__ acc, const R AB[3],
 // One thread per shell quartet of an L <= 4 class, Obara-Saika integrals.
 // R as in eri_reg_kernel: double, or float for the FP32 list (the Boys
 // values and the per-primitive scalars stay FP64).  MINB: blocks of 128 per
-// SM the register allocation must allow (1: the compiler's choice; 4: at
-// most 128 registers, for the autotuner to weigh occupancy against spills).
+// SM the register allocation must allow (1: the compiler's choice; the
+// denser build of each class asks for 8, 6 or 4, at most 64, 80 or 128
+// registers, for the autotuner to weigh occupancy against spills).
 template <int LA, int LB, int LC, int LD, int NK, typename R = double, int MINB = 1>
 __global__ void __launch_bounds__(128, MINB) eri_os_kernel(const uint2 *__restrict__ quartets, long long nq, JKArgs args)
 {
