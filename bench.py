@@ -119,15 +119,16 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU path: the oracle's streaming restatement of the reference's direct build
 # ---------------------------------------------------------------------------
-def cpu_fock_rate(shells, budget_s=12.0, seed=SEED):
+def cpu_fock_rate(shells, rows=4096, seed=SEED):
     """Fock builds/s of the reference's direct path on the host cores,
-    extrapolated from a stratified sample of bra AO-pair rows.  Per build the
-    reference recomputes the Schwarz table serially (os.cpp:1447, timed in
-    full here) and evaluates every screened canonical AO quartet with its
-    per-component OS code (os.cpp:1458-1507, restated); its nb^4 tensor
-    scatter and O(nb^4) digestion (os.cpp:1450, 1514-1520) cannot run at 800
-    functions (3.3 TB) and are replaced by the streaming digestion, which only
-    makes the baseline faster."""
+    extrapolated from a stratified sample of `rows` bra AO-pair rows (one row
+    drawn per stratum with a fixed seed, so every call times the same rows).
+    Per build the reference recomputes the Schwarz table serially
+    (os.cpp:1447, timed in full here) and evaluates every screened canonical
+    AO quartet with its per-component OS code (os.cpp:1458-1507, restated);
+    its nb^4 tensor scatter and O(nb^4) digestion (os.cpp:1450, 1514-1520)
+    cannot run at 800 functions (3.3 TB) and are replaced by the streaming
+    digestion, which only makes the baseline faster."""
     import oracle
     ob = oracle.Basis(shells)
     nb, npairs = ob.nbasis, ob.npairs
@@ -136,27 +137,21 @@ def cpu_fock_rate(shells, budget_s=12.0, seed=SEED):
     t_schwarz = time.perf_counter() - t0
     Pm = density(nb)
     rng = np.random.default_rng(seed)
-
-    def sample(strata):
-        edges = np.linspace(0, npairs, strata + 1).astype(np.int64)
-        rows = np.array([rng.integers(edges[i], max(edges[i] + 1, edges[i + 1])) for i in range(strata)],
-                        dtype=np.int32)
-        t = time.perf_counter()
-        _, _, n = ob.jk_direct_rows(Pm, [Pm], rows, 1e-10, oracle.OS, Q=Q)
-        dt = time.perf_counter() - t
-        return dt * npairs / strata, n * npairs / strata, dt, n, strata
-
-    est, nq, dt, n, s = sample(32)
-    strata = int(min(npairs, max(32, 32 * (budget_s - dt) / max(dt, 1e-3))))
-    if strata > 32 and dt < budget_s:
-        est, nq, dt, n, s = sample(strata)
-    t_build = t_schwarz + est
+    strata = int(min(npairs, rows))
+    edges = np.linspace(0, npairs, strata + 1).astype(np.int64)
+    picks = np.array([rng.integers(edges[i], max(edges[i] + 1, edges[i + 1])) for i in range(strata)],
+                     dtype=np.int32)
+    t = time.perf_counter()
+    _, _, n = ob.jk_direct_rows(Pm, [Pm], picks, 1e-10, oracle.OS, Q=Q)
+    dt = time.perf_counter() - t
+    t_build = t_schwarz + dt * npairs / strata
+    nq = n * npairs / strata
     return {"value": 1.0 / t_build, "unit": "Fock builds/s", "cores": oracle.lib().orc_num_threads(),
             "kind": "port",
-            "sample": f"{s} stratified bra rows of {npairs} ({n} of ~{nq:.3g} screened AO quartets) in "
-                      f"{dt:.1f}s + full serial Schwarz table {t_schwarz:.1f}s; build time extrapolated to "
-                      f"{t_build:.0f}s",
-            "est_seconds_per_build": t_build}
+            "sample": f"{strata} stratified bra rows of {npairs} (fixed seed {seed}; {n} of ~{nq:.3g} screened AO "
+                      f"quartets) in {dt:.1f}s + full serial Schwarz table {t_schwarz:.1f}s; build time "
+                      f"extrapolated to {t_build:.0f}s",
+            "sample_seconds": dt + t_schwarz, "est_seconds_per_build": t_build}
 
 
 def reference_arm(args):
@@ -166,10 +161,10 @@ def reference_arm(args):
     atoms, mol, shells = build_shells()
     vals = []
     for _ in range(args.warmup):
-        cpu_fock_rate(shells, budget_s=2.0)
+        cpu_fock_rate(shells, rows=256)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_fock_rate(shells, budget_s=args.ref_budget))
+        vals.append(cpu_fock_rate(shells, rows=args.cpu_rows))
     wall = time.perf_counter() - t0
     v = float(np.mean([x["value"] for x in vals]))
     line = {"metric": "Fock builds/s", "value": v, "unit": "Fock builds/s", "impl": "reference",
@@ -180,10 +175,13 @@ def reference_arm(args):
             "cpu_baseline": {"value": v, "unit": "Fock builds/s", "cores": vals[-1]["cores"], "kind": "port",
                              "sample": vals[-1]["sample"]},
             "e2e": {"value": v, "unit": "Fock builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall,
+            "wall_s": wall, "extrapolated": True,
+            "sample_seconds_per_step": wall / max(1, args.steps),
             "note": "the reference's own direct build materialises an nb^4 tensor (3.3 TB at 800 functions) "
                     "and cannot run; timed is the oracle's restatement of its integral path with streaming "
-                    "digestion on all host threads"}
+                    "digestion on all host threads, on the same fixed sample of bra rows every step, and "
+                    "value / ms_per_step are that sample's time extrapolated to the whole build (each step "
+                    "takes sample_seconds_per_step of wall time)"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -393,14 +391,15 @@ def ours_arm(args):
     # end to end through the C ABI with host buffers (pinned), per step:
     # H2D of P, build, D2H of G (+ the all-reduce of the partial G when N > 1)
     Ph = torch.from_numpy(Pm).pin_memory().numpy()
+    Gpin = torch.empty(Pm.shape, dtype=torch.float64).pin_memory().numpy()
     Gacc = torch.zeros_like(dP)
     for _ in range(2):
-        eng.fock_rhf(Ph)
+        eng.fock_rhf(Ph, out=Gpin)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        Gh = eng.fock_rhf(Ph)
+        Gh = eng.fock_rhf(Ph, out=Gpin)
         if world > 1:
             Gacc.copy_(torch.from_numpy(Gh))
             dist.all_reduce(Gacc)
@@ -506,7 +505,7 @@ def ours_arm(args):
         if mixed:
             line["mixed_precision"] = mixed
         if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = {k: v for k, v in cpu_fock_rate(shells, budget_s=args.cpu_budget).items()
+            line["cpu_baseline"] = {k: v for k, v in cpu_fock_rate(shells, rows=args.cpu_rows).items()
                                     if k != "est_seconds_per_build"}
         if world == 1 and not args.no_scf:
             # in a child process that never imports torch, as a C++ host would
@@ -773,8 +772,8 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="mixed: FP32 below a Schwarz bound of 1e-8 (the benchmark configuration); "
                          "the all-FP64 build is timed beside it")
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU sampling for cpu_baseline")
-    ap.add_argument("--ref-budget", type=float, default=8.0, help="seconds of CPU sampling per reference step")
+    ap.add_argument("--cpu-rows", type=int, default=4096,
+                    help="bra AO-pair rows the CPU baseline and each reference step time (the same rows every time)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-scf", action="store_true", help="skip the C40H82 time-to-energy leg")
     ap.add_argument("--lanes", type=int, default=4, choices=[1, 2, 3, 4],

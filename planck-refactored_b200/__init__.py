@@ -198,11 +198,17 @@ class FockEngine:
         self._check(self.lib.pfk_quartet_list(self.h, _p(out), n_ao, ctypes.byref(n)))
         return out[:n.value]
 
-    def fock_rhf(self, P):
+    def fock_rhf(self, P, out=None):
+        """G = J(P) - K(P)/2 from host buffers (pfk_fock_rhf).  out: an
+        optional C-contiguous float64 host array for G (pinned memory makes
+        the device-to-host copy a single DMA); a new array otherwise."""
         P = _f64(P)
-        G = np.zeros_like(P)
-        self._check(self.lib.pfk_fock_rhf(self.h, _p(P), _p(G)))
-        return G
+        if out is None:
+            out = np.empty_like(P)   # every element is written
+        elif out.dtype != np.float64 or out.shape != P.shape or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a C-contiguous float64 array shaped like P")
+        self._check(self.lib.pfk_fock_rhf(self.h, _p(P), _p(out)))
+        return out
 
     def fock_uhf(self, Pa, Pb):
         Pa, Pb = _f64(Pa), _f64(Pb)

@@ -216,3 +216,26 @@ def test_larger_systems_quartet_set_and_fock():
         J_o, K_o, _ = ob.jk_direct(Pm, [Pm], 1e-10, oracle.OS, Q=Qo)
         G_o = J_o - 0.5 * K_o[0]
         assert np.abs(eng.fock_rhf(Pm) - G_o).max() < 1e-10
+
+
+def test_rejects_asymmetric_and_nonfinite_density(water):
+    """pfk_fock_rhf checks its density on the host before any device work:
+    asymmetric (above 1e-10 relative) or non-finite densities fail with
+    PFK_ERR_INVALID and a message; a density asymmetric at the rounding level
+    is accepted."""
+    P = pfk()
+    eng = water[0]
+    Pm = random_density(eng.nbasis, seed=3)
+    G = eng.fock_rhf(Pm)
+    Pn = Pm.copy()
+    Pn[0, 1] += 1e-15
+    assert np.abs(eng.fock_rhf(Pn) - G).max() < 1e-12
+    for bad in ("asym", "nan", "inf"):
+        Pb = Pm.copy()
+        if bad == "asym":
+            Pb[3, 7] += 1e-6
+        else:
+            Pb[5, 5] = np.nan if bad == "nan" else np.inf
+        with pytest.raises(P.PfkError) as e:
+            eng.fock_rhf(Pb)
+        assert e.value.status == 1 and "not symmetric" in str(e.value)
