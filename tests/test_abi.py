@@ -188,3 +188,41 @@ def test_contexts_do_not_leak_device_memory():
         eng.close()
     torch.cuda.synchronize()
     assert free0 - torch.cuda.mem_get_info()[0] < 8 << 20
+
+
+def test_header_compiles_and_links_as_c(tmp_path):
+    """A C99 caller (-pedantic -Werror) includes include/planck_fock.h, takes
+    the address of every function it declares, links against the library and
+    runs its argument checks: the header is plain C and every declaration
+    resolves to the library's symbol of the same name."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    syms = declared_symbols()
+    src = tmp_path / "abi_check.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "planck_fock.h"\n'
+        "typedef void (*fn)(void);\n"
+        "int main(void) {\n"
+        "    volatile fn all[] = {" + ", ".join(f"(fn){s}" for s in syms) + "};\n"
+        "    pfk_ctx *ctx = NULL;\n"
+        "    size_t i;\n"
+        "    for (i = 0; i < sizeof all / sizeof all[0]; ++i)\n"
+        "        if (!all[i]) return 2;\n"
+        "    if (pfk_create(NULL, 0, &ctx) != PFK_ERR_INVALID || ctx != NULL) return 3;\n"
+        "    if (strlen(pfk_last_error(NULL)) == 0) return 4;\n"
+        "    puts(pfk_last_error(NULL));\n"
+        "    return 0;\n}\n")
+    lib_dir = os.path.dirname(pfk().LIB_PATH)
+    exe = tmp_path / "abi_check"
+    r = subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Werror", "-I",
+                        os.path.join(REPO, "include"), str(src), "-L", lib_dir, "-lplanck_fock",
+                        "-Wl,-rpath," + lib_dir, "-Wl,-rpath-link,/usr/local/cuda/lib64", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    env = dict(os.environ, LD_LIBRARY_PATH=":".join(filter(None, ["/usr/local/cuda/lib64",
+                                                                  os.environ.get("LD_LIBRARY_PATH", "")])))
+    r = subprocess.run([str(exe)], capture_output=True, text=True, env=env)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert "null" in r.stdout
