@@ -43,7 +43,8 @@ thread_local std::string g_mlp_error;
 // thread waits on before the tiles are overwritten.  The epilogue reads the
 // accumulator back with tcgen05.ld, warp w taking rows 32w .. 32w+31 (the
 // tensor-memory lanes a warp may access).  Waits are bounded (2 s of
-// %globaltimer); a wait that runs out sets *err and the CTA stops issuing.
+// %globaltimer); a wait that runs out sets *err, the CTA stops issuing,
+// waits (bounded again) for the round in flight and frees its columns.
 // ---------------------------------------------------------------------------
 constexpr int TC_M = 128, TC_N = 64, TC_K = 64;
 constexpr int TC_A_BYTES = TC_M * TC_K * 2, TC_B_BYTES = TC_N * TC_K * 2;
@@ -208,6 +209,9 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int M, int N, int K, const
 
     if (failed) {
         if (tid == 0) atomicExch(err, 1);
+        // the round whose wait ran out may still complete: wait for it once
+        // more (bounded) before its accumulator columns are released below
+        tc_wait(sbar, parity ^ 1u);
     } else {
         const int m = m0 + warp * 32 + lane;
 #pragma unroll 1
