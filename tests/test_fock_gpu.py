@@ -1,6 +1,6 @@
 """Parity of the CUDA Fock engine with the oracle (GPU tests).
 
-Tolerances (north star): integrals within 1e-10 absolute on the FP64 path;
+Tolerances (the project's accuracy targets): integrals within 1e-10 absolute on the FP64 path;
 G/J/K within 1e-10 absolute; converged energies within 1e-8 Eh of the oracle
 and within the reference's own 1e-9 of its regression energies.  Screened
 quartet sets must be identical (count and digest)."""

@@ -2,8 +2,8 @@
 fp32_bound run with FP32 2D integrals, transfers and contraction; roots,
 weights, screening and J/K accumulation stay FP64.  The error against the
 all-FP64 build is stated here: G within 1e-9 absolute and converged SCF
-energies within 1e-6 Eh (the north-star bound for mixed precision; observed
-errors are orders of magnitude smaller)."""
+energies within 1e-6 Eh (the accuracy bound this project sets for mixed
+precision; observed errors are orders of magnitude smaller)."""
 import numpy as np
 import pytest
 
