@@ -486,7 +486,7 @@ def ours_arm(args):
                              "traffic": _traffic_from_profiles(top[0])[0],
                              "traffic_source": _traffic_from_profiles(top[0])[1],
                              "peak_source": "FP64 FMA loop measured in this run (pfk_measure_fma_peak); "
-                                            "the driver's peaks file lists HBM and BF16 only",
+                                            "the measured-peaks file lists HBM copy and BF16 GEMM peaks only",
                              "flops_per_launch": top_flops, "launch_ms": top[1][2]},
                 "roofline_build": {"achieved": build_ach, "peak": fp64_peak, "unit": "TFLOP/s",
                                    "frac": build_ach / fp64_peak, "flops_per_build": flops},

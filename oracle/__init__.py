@@ -3,7 +3,7 @@
 This package restates the reference's algorithm on the CPU (oracle.c, built
 into liboracle.so with gcc + OpenMP) and drives it from Python.  Only tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm may import
-it, and only as the checker: the product path never routes through it.
+it, and only to compare against: the product path never routes through it.
 
 Pinned against (tests/test_oracle.py):
   * the reference's own Boys function (src/lookup/boys.cpp compiled unmodified,

@@ -1,6 +1,6 @@
 """CPU restatement of the reference's checkpoint format (test infrastructure).
 
-This is the checker for the library's .hfchk writer and density reader
+The tests compare the library's .hfchk writer and density reader with it
 (planck-refactored_b200/csrc/pfk_checkpoint.cu); nothing in the product
 imports it.  It follows the reference's src/io/checkpoint.cpp:
   save()                      checkpoint.cpp:347-489

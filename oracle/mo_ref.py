@@ -1,6 +1,6 @@
 """CPU restatement of the reference's AO -> MO transform and MP2 energies
-(test infrastructure: the checker for pfk_mo_transform and
-planck-refactored_b200/mp2.py; nothing in the product imports it).
+(test infrastructure: the tests compare pfk_mo_transform and
+planck-refactored_b200/mp2.py with it; nothing in the product imports it).
 
   transform_eri  src/post_hf/integrals.cpp:63-134 -- four quarter
                  transforms over a row-major nb^4 AO tensor, each a

@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this file;
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
- * use it as the checker.  Each function cites the reference file:line it
+ * use it as the reference to compare against.  Each function cites the reference file:line it
  * restates (paths relative to the reference project root).
  *
  * Parity pins (tests/test_oracle.py):
