@@ -1372,7 +1372,7 @@ pfk_status pfk_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tf
 //
 // For callers that may not allocate device memory -- code that runs inside a
 // host application whose GPU memory is owned by another allocator or pool,
-// or whose memory budget is fixed up front -- every device buffer this build
+// or whose memory budget is fixed up front -- every device buffer the build
 // needs (shell-pair and primitive-pair data, the Schwarz table, the screened
 // quartet list, the J and K accumulators) is carved out of one file-scope
 // array of PFK_NOALLOC_SCRATCH_BYTES.  Every GPU that loads this library
